@@ -1,0 +1,304 @@
+#!/usr/bin/env python3
+"""Benchmark of the PoSE-DB labeling hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload plain_2e17|plain_small|window_2e17]
+
+One step = one pass of the hot path over one batch: label the workload's
+super-chunks (default: 32 consecutive super-chunks at chunk_blocks = 2^17,
+key splitmix64(1) — the plain drop-in at write-up depth) through the C ABI
+pose_graph_hbm_topo_label with the topology resident, as disk-wipe-bench's
+worker does per HBM window.  Metric: persisted label MiB/s
+(chunk_blocks*32 bytes per super-chunk / time), the reference's own
+definition (common/src/cuda/label_gpu_common.cu:312-315).
+
+Under torchrun each rank labels its own disjoint range of super-chunks
+(absolute positions offset by rank): no collective on the data path, weak
+scaling; the step time is the max over ranks.
+
+--impl reference times the reference's own CPU labeler
+(pose_graph_label_region_pooled_inplace, built from source into oracle/_ref)
+on this host's cores on a bounded sample of the same workload; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "pose-memory-wiping_b200")
+MIB = float(1 << 20)
+
+
+def load_pkg():
+    if "pose_b200" in sys.modules:
+        return sys.modules["pose_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "pose_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["pose_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload(name: str) -> dict:
+    import pose_b200.workloads as wl
+    if name == "plain_2e17":
+        w = wl.plain_2e17()
+    elif name == "plain_small":
+        w = wl.plain_small()
+    elif name == "window_2e17":
+        # the reference's default 16 GiB HBM window at 2^17 (4096 super-chunks)
+        w = dict(wl.plain_2e17(), name="window_2e17", chunks=4096)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    w["nodes_per_chunk"] = wl.chunk_nodes(w["chunk_blocks"])
+    return w
+
+
+# ── clocks ──────────────────────────────────────────────────────────────────
+
+CLOCK_Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+class ClockSampler:
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = f"/tmp/.pose_b200_clocks_{os.getpid()}_{gpu_index}.csv"
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={CLOCK_Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for ln in open(self.path):
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = sorted(sm)[len(sm) // 2:] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ── reference CPU leg ───────────────────────────────────────────────────────
+
+def cpu_reference(w: dict, steps: int, warmup: int, cores: int | None = None) -> dict:
+    """Time the reference's own CPU in-place labeler (oracle/_ref) on a
+    bounded sample: one super-chunk per host thread per step."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import RefCPU  # test-infrastructure checker, CPU legs only
+    ref = RefCPU()
+    cores = cores or os.cpu_count() or 1
+    cb = w["chunk_blocks"]
+    n = min(w["chunks"], cores)
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        ref.label_super_chunks(w["key"], cb, n, w["rbo"], threads=cores)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+    sec = sum(times) / len(times)
+    return {"value": n * cb * 32 / MIB / sec, "unit": "MiB/s", "cores": cores, "kind": "reference",
+            "sample": f"{n} super-chunks of chunk_blocks={cb} per step ({n * w['nodes_per_chunk']:.3g} nodes), "
+                      f"{steps} timed steps, one chunk per host thread",
+            "seconds_per_step": sec}
+
+
+def run_reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    load_pkg()
+    w = workload(args.workload)
+    steps = max(1, min(args.steps, 3))
+    warm = 1 if args.warmup > 0 else 0
+    cb = cpu_reference(w, steps, warm)
+    line = {"metric": "label MiB/s (persisted output-set bytes / time)", "value": cb["value"],
+            "unit": "MiB/s", "n_gpus": args.gpus, "steps": steps, "warmup": warm,
+            "ms_per_step": cb["seconds_per_step"] * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (splitmix64 session keys)",
+            "impl": "reference",
+            "config": {"workload": w["name"], "chunk_blocks": w["chunk_blocks"], "super_chunks": w["chunks"],
+                       "parallelism": "host threads"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "MiB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ── B200 arm ────────────────────────────────────────────────────────────────
+
+def run_b200(args) -> None:
+    import torch
+    pkg = load_pkg()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    os.environ.setdefault("POSE_GPU_QUIET", "1")
+    w = workload(args.workload)
+    cb, nsup = w["chunk_blocks"], w["chunks"]
+    sb = cb * 32
+    nbytes = nsup * sb
+    rbo = w["rbo"] + rank * nsup * cb  # each rank: its own disjoint absolute range
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    topo = pkg.Topology(cb, cv0_table=not args.no_cv0)
+    buf = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+
+    # roofline denominator: the GPU's compression rate for this instruction mix
+    rate, lat_cycles = pkg.compress_rate(2048)
+
+    for _ in range(args.warmup):
+        rc = topo.label(w["key"], buf.data_ptr(), nbytes, rbo)
+        assert rc == 0, pkg.last_error()
+
+    stats = []
+    barrier()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            rc, st = topo.label(w["key"], buf.data_ptr(), nbytes, rbo, stats=True)
+            assert rc == 0, pkg.last_error()
+            stats.append(st)
+        barrier()
+        # end to end through the public API with host buffers: the session key
+        # goes host->device inside the call, the persisted labels come back
+        # into pinned host memory
+        e2e_times = []
+        for _ in range(max(1, args.steps)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rc = topo.label(w["key"], buf.data_ptr(), nbytes, rbo)
+            host.copy_(buf, non_blocking=False)
+            torch.cuda.synchronize()
+            e2e_times.append(time.perf_counter() - t0)
+            assert rc == 0
+        barrier()
+    device_ms = sum(s["total_ms"] for s in stats)
+    kernel_ms = sum(s["kernel_ms"] for s in stats) / len(stats)
+    e2e_s = sum(e2e_times) / len(e2e_times)
+    if dist:
+        t = torch.tensor([device_ms, e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        device_ms, e2e_s = float(t[0]), float(t[1])
+    ms_per_step = device_ms / args.steps
+    value = world * nbytes / MIB / (ms_per_step * 1e-3)
+    e2e_value = world * nbytes / MIB / e2e_s
+    st0 = stats[0]
+    comps = 2 if st0["used_cv0_table"] else 3
+    nodes = st0["nodes"]
+    ops_per_compress = 680.0  # 7 rounds x 8 G x 12 int32 ops + 8 output xors
+    achieved_ops = nodes * comps * ops_per_compress / (kernel_ms * 1e-3)
+    peak_ops = rate * ops_per_compress
+    info = topo.info()
+    levels = info["levels"]
+    clocks = clk.summary()
+    # depth bound: one label per level on the critical path, each ~comps
+    # dependent compressions at the measured compression latency
+    sm_hz = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    t_depth = levels * comps * lat_cycles / sm_hz
+    line = {
+        "metric": "label MiB/s (persisted output-set bytes / time)",
+        "value": value, "unit": "MiB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic (splitmix64 session keys)", "impl": "b200",
+        "config": {"workload": w["name"], "chunk_blocks": cb, "super_chunks": nsup,
+                   "nodes_per_step": nsup * w["nodes_per_chunk"], "parallelism": f"chunk-sharded x{world}",
+                   "l2": "inputs larger than L2 (topology store %.2f GB read per step)" % (info["device_bytes"] / 1e9),
+                   "schedule": {"T": st0["team_warps"], "G": st0["units_per_team"], "teams": st0["teams"]},
+                   "cv0_table": bool(st0["used_cv0_table"])},
+        "roofline": {"bound": "int32", "achieved": achieved_ops / 1e12, "peak": peak_ops / 1e12,
+                     "unit": "Tops/s", "frac": achieved_ops / peak_ops, "traffic": None,
+                     "peak_source": "measured in this run: k_compress_bench (every SM full, register-resident compressions)",
+                     "ops_per_node": comps * ops_per_compress,
+                     "spec_ops_per_node": 3 * ops_per_compress,
+                     "depth_bound_mib_s": nsup * sb / MIB / t_depth if t_depth > 0 else None,
+                     "depth_frac": (t_depth * 1e3) / kernel_ms if kernel_ms > 0 else None,
+                     "compress_latency_cycles": lat_cycles},
+        "e2e": {"value": e2e_value, "unit": "MiB/s", "h2d_bytes_per_step": len(w["key"]),
+                "d2h_bytes_per_step": nbytes},
+        "gpu_launches": int(sum(2 * s["kernel_launches"] for s in stats)),
+        "clocks": clocks,
+        "kernel_ms": kernel_ms,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference(w, 1, 0)
+            line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as exc:  # the checker build may be absent
+            line["cpu_baseline"] = {"value": None, "unit": "MiB/s", "cores": os.cpu_count(), "kind": "reference",
+                                    "sample": f"unavailable: {exc}"}
+    topo.free()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="plain_2e17")
+    ap.add_argument("--no-cv0", action="store_true", help="hash block 0 in every call (no table)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,78 @@
+/*
+ * pose_b200.h — additive C ABI of the B200 labeler (libpose_b200.so).
+ *
+ * New symbols next to the drop-in ones in gpu_label.h; none of them changes
+ * the behaviour of the drop-in entry points.  The reference has no
+ * counterpart for the schedule/statistics structs; each function below names
+ * the reference interface it extends.
+ */
+#ifndef POSE_B200_H
+#define POSE_B200_H
+
+#include "gpu_label.h"
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Schedule of one labeling launch.  Zero fields mean "choose automatically". */
+typedef struct {
+    uint32_t team_warps;        /* T: warps that cooperate on one batch (1..16, power of 2) */
+    uint32_t units_per_team;    /* G: chunk copies run in lockstep by one team (1..32, power of 2) */
+    uint32_t max_teams;         /* cap on resident teams (0 = occupancy and memory bound) */
+    uint32_t reserved;
+    uint64_t scratch_cap_bytes; /* cap on the scratch pool (0 = free HBM less a margin) */
+} pose_b200_sched_t;
+
+/* What one call did (device times from CUDA events on the labeler's stream). */
+typedef struct {
+    double kernel_ms;           /* labeling kernel(s) */
+    double total_ms;            /* whole call on the device stream (seeds, kernel, zeroing) */
+    uint64_t super_chunks;      /* super-chunks labelled */
+    uint64_t units;             /* chunk copies (2 per super-chunk unless chunk_blocks == 1) */
+    uint64_t nodes;             /* node labels computed */
+    uint64_t scratch_bytes;     /* scratch pool bytes used */
+    uint32_t team_warps, units_per_team, teams, kernel_launches;
+    uint32_t used_cv0_table;    /* 1 when block 0 came from the precomputed table */
+    uint32_t reserved;
+} pose_b200_stats_t;
+
+/* Extends pose_graph_hbm_topo_build (common/include/gpu_label.h:77-78).
+ * with_cv0_table: 1 = also build the block-0 chaining-value table
+ * (copies * nodes * 32 bytes of HBM), 0 = hash block 0 in every label call. */
+pose_hbm_topo_t *pose_b200_topo_build(uint32_t chunk_blocks, int with_cv0_table);
+
+/* Extends pose_graph_hbm_topo_label (common/include/gpu_label.h:80-83) with an
+ * explicit schedule (NULL = automatic) and statistics (NULL = none).  Same
+ * bytes, same return convention, synchronous. */
+int pose_b200_topo_label(const pose_hbm_topo_t *topo, const uint8_t *session_seed,
+                         size_t seed_len, void *hbm_dev_ptr, size_t hbm_len,
+                         uint64_t region_block_offset, const pose_b200_sched_t *sched,
+                         pose_b200_stats_t *stats);
+
+/* Topology facts (any pointer may be NULL). */
+void pose_b200_topo_info(const pose_hbm_topo_t *topo, uint32_t *chunk_blocks,
+                         uint64_t *nodes_per_chunk, uint32_t *levels, uint32_t *pool_slots,
+                         uint64_t *device_bytes);
+
+/* The schedule the automatic policy would pick for `units` chunk copies. */
+int pose_b200_plan(const pose_hbm_topo_t *topo, uint64_t super_chunks,
+                   const pose_b200_sched_t *hint, pose_b200_sched_t *out);
+
+/* Sustained compression rate of this GPU for the labeler's instruction mix:
+ * every SM full of threads chaining register-resident compressions.  Returns
+ * compressions per second (0 on error); *latency_cycles gets the dependent
+ * latency of one compression in SM clocks (NULL to skip). */
+double pose_b200_compress_rate(uint32_t iters, double *latency_cycles);
+
+/* Last error message of the calling thread ("" when none). */
+const char *pose_b200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POSE_B200_H */

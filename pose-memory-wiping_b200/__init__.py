@@ -1,0 +1,222 @@
+"""pose_b200 — Python host mirror of the reference's GPU labeler C API.
+
+The product is ``libpose_b200.so`` (C11 host code + sm_100a kernels, built
+from ``csrc/`` by the Makefile next to this file).  This module is a thin
+ctypes layer over its C ABI (``include/gpu_label.h``, ``include/pose_b200.h``)
+with the reference's names, argument meaning and error behaviour
+(Amodo-Design/PoSE-Memory-Wiping, ``common/include/gpu_label.h:40-100``):
+entry points return 0 / -1 (``None`` for a failed topology build) and print
+their error to stderr.  Device buffers are raw device pointers (integers);
+tests and the bench obtain them from torch, which is only plumbing here.
+
+There is no CPU fallback: if the library cannot be loaded, ``load()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpose_b200.so")
+INCLUDE_DIR = os.path.join(os.path.dirname(HERE), "include")
+
+POSE_HASH_BLAKE3 = 0
+POSE_HASH_SHA256 = 1
+POSE_HASH_AES_PRF = 2
+POSE_CHUNK_BLOCKS = 4096
+POSE_GRAPH_MAX_M = 1 << 20
+
+_lib = None
+_lock = threading.Lock()
+
+
+class Sched(C.Structure):
+    """pose_b200_sched_t: zero fields mean automatic."""
+
+    _fields_ = [("team_warps", C.c_uint32), ("units_per_team", C.c_uint32),
+                ("max_teams", C.c_uint32), ("reserved", C.c_uint32),
+                ("scratch_cap_bytes", C.c_uint64)]
+
+
+class Stats(C.Structure):
+    """pose_b200_stats_t."""
+
+    _fields_ = [("kernel_ms", C.c_double), ("total_ms", C.c_double),
+                ("super_chunks", C.c_uint64), ("units", C.c_uint64), ("nodes", C.c_uint64),
+                ("scratch_bytes", C.c_uint64), ("team_warps", C.c_uint32),
+                ("units_per_team", C.c_uint32), ("teams", C.c_uint32),
+                ("kernel_launches", C.c_uint32), ("used_cv0_table", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_u8p = C.POINTER(C.c_uint8)
+_u32p = C.POINTER(C.c_uint32)
+
+
+def build(force: bool = False) -> str:
+    """Compile libpose_b200.so in place (nvcc for sm_100a + gcc)."""
+    args = ["make", "-s", "-C", HERE]
+    if force:
+        subprocess.run(args + ["clean"], check=True)
+    subprocess.run(args, check=True)
+    return LIB_PATH
+
+
+def _declare(L: C.CDLL) -> None:
+    L.pose_graph_label_hbm.argtypes = [_u8p, C.c_size_t, C.c_uint32, C.c_void_p, C.c_size_t,
+                                       C.c_uint64, C.c_int]
+    L.pose_graph_label_hbm.restype = C.c_int
+    L.pose_graph_hbm_topo_build.argtypes = [C.c_uint32, C.c_int]
+    L.pose_graph_hbm_topo_build.restype = C.c_void_p
+    L.pose_graph_hbm_topo_label.argtypes = [C.c_void_p, _u8p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                            C.c_uint64]
+    L.pose_graph_hbm_topo_label.restype = C.c_int
+    L.pose_graph_hbm_topo_free.argtypes = [C.c_void_p]
+    L.pose_graph_hbm_topo_free.restype = None
+    L.pose_gpu_label_node_single.argtypes = [_u8p, C.c_int, C.c_uint64, _u8p, _u8p, _u8p, _u8p,
+                                             _u32p, _u32p]
+    L.pose_gpu_label_node_single.restype = C.c_int
+    L.pose_b200_topo_build.argtypes = [C.c_uint32, C.c_int]
+    L.pose_b200_topo_build.restype = C.c_void_p
+    L.pose_b200_topo_label.argtypes = [C.c_void_p, _u8p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                       C.c_uint64, C.POINTER(Sched), C.POINTER(Stats)]
+    L.pose_b200_topo_label.restype = C.c_int
+    L.pose_b200_topo_info.argtypes = [C.c_void_p, _u32p, C.POINTER(C.c_uint64), _u32p, _u32p,
+                                      C.POINTER(C.c_uint64)]
+    L.pose_b200_topo_info.restype = None
+    L.pose_b200_plan.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(Sched), C.POINTER(Sched)]
+    L.pose_b200_plan.restype = C.c_int
+    L.pose_b200_compress_rate.argtypes = [C.c_uint32, C.POINTER(C.c_double)]
+    L.pose_b200_compress_rate.restype = C.c_double
+    L.pose_b200_last_error.argtypes = []
+    L.pose_b200_last_error.restype = C.c_char_p
+
+
+def load() -> C.CDLL:
+    """Load the in-tree library, building it first if it is missing."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                build()
+            L = C.CDLL(LIB_PATH)
+            _declare(L)
+            _lib = L
+    return _lib
+
+
+def _bytes_arg(b: bytes | None):
+    if b is None:
+        return None
+    return C.cast(C.create_string_buffer(bytes(b), max(1, len(b))), _u8p)
+
+
+def last_error() -> str:
+    return load().pose_b200_last_error().decode(errors="replace")
+
+
+class Topology:
+    """A resident topology (pose_hbm_topo_t) for one chunk_blocks value."""
+
+    def __init__(self, chunk_blocks: int, algo: int = POSE_HASH_BLAKE3, cv0_table: bool = True):
+        L = load()
+        if algo != POSE_HASH_BLAKE3:
+            h = L.pose_graph_hbm_topo_build(chunk_blocks, algo)
+        else:
+            h = L.pose_b200_topo_build(chunk_blocks, 1 if cv0_table else 0)
+        if not h:
+            raise RuntimeError(f"topology build failed: {last_error()}")
+        self.handle = h
+        self.chunk_blocks = chunk_blocks or POSE_CHUNK_BLOCKS
+        self.super_bytes = self.chunk_blocks * 32
+
+    def info(self) -> dict:
+        cb = C.c_uint32()
+        nodes = C.c_uint64()
+        lv = C.c_uint32()
+        pool = C.c_uint32()
+        dev = C.c_uint64()
+        load().pose_b200_topo_info(self.handle, C.byref(cb), C.byref(nodes), C.byref(lv),
+                                   C.byref(pool), C.byref(dev))
+        return {"chunk_blocks": cb.value, "nodes_per_chunk": nodes.value, "levels": lv.value,
+                "pool_slots": pool.value, "device_bytes": dev.value}
+
+    def label(self, seed: bytes, dev_ptr: int, nbytes: int, region_block_offset: int = 0,
+              sched: Sched | None = None, stats: bool = False):
+        """pose_graph_hbm_topo_label (or the scheduled variant).  Returns the
+        C return code, or (rc, stats dict) when stats=True."""
+        L = load()
+        if sched is None and not stats:
+            return L.pose_graph_hbm_topo_label(self.handle, _bytes_arg(seed), len(seed),
+                                               C.c_void_p(dev_ptr), nbytes, region_block_offset)
+        st = Stats()
+        rc = L.pose_b200_topo_label(self.handle, _bytes_arg(seed), len(seed), C.c_void_p(dev_ptr),
+                                    nbytes, region_block_offset,
+                                    C.byref(sched) if sched is not None else None, C.byref(st))
+        return (rc, st.as_dict()) if stats else rc
+
+    def plan(self, super_chunks: int, hint: Sched | None = None) -> Sched | None:
+        out = Sched()
+        rc = load().pose_b200_plan(self.handle, super_chunks,
+                                   C.byref(hint) if hint is not None else None, C.byref(out))
+        return out if rc == 0 else None
+
+    def free(self) -> None:
+        if self.handle:
+            load().pose_graph_hbm_topo_free(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.free()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def label_hbm(seed: bytes, chunk_blocks: int, dev_ptr: int, nbytes: int,
+              region_block_offset: int = 0, algo: int = POSE_HASH_BLAKE3) -> int:
+    """pose_graph_label_hbm: build, label, free."""
+    return load().pose_graph_label_hbm(_bytes_arg(seed), len(seed), chunk_blocks, C.c_void_p(dev_ptr),
+                                       nbytes, region_block_offset, algo)
+
+
+def label_node_single(is_source: int, node_index: int, pred0: bytes | None, pred1: bytes | None,
+                      seed: bytes, descriptor: bytes, key_src, key_int) -> bytes | None:
+    """pose_gpu_label_node_single; returns the 32-byte label or None on error."""
+    out = (C.c_uint8 * 32)()
+    ks = (C.c_uint32 * 8)(*[int(x) for x in key_src])
+    ki = (C.c_uint32 * 8)(*[int(x) for x in key_int])
+    rc = load().pose_gpu_label_node_single(C.cast(out, _u8p), int(is_source), node_index,
+                                           _bytes_arg(pred0), _bytes_arg(pred1), _bytes_arg(seed),
+                                           _bytes_arg(descriptor), C.cast(ks, _u32p), C.cast(ki, _u32p))
+    return bytes(out) if rc == 0 else None
+
+
+def compress_rate(iters: int = 4096) -> tuple[float, float]:
+    """(compressions/s with every SM full, dependent cycles per compression)."""
+    lat = C.c_double()
+    rate = load().pose_b200_compress_rate(iters, C.byref(lat))
+    return rate, lat.value
+
+
+def exported_symbols() -> list[str]:
+    """Function names declared in include/*.h (the C ABI this library promises)."""
+    import re
+    names = []
+    for fn in sorted(os.listdir(INCLUDE_DIR)):
+        if fn.endswith(".h"):
+            src = open(os.path.join(INCLUDE_DIR, fn)).read()
+            src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+            names += re.findall(r"\b(pose_[a-z0-9_]+)\s*\(", src)
+    return sorted(set(names))

@@ -1,0 +1,72 @@
+/* kernels.h — the thin C-ABI between the C11 host code and the sm_100a
+ * kernels in label_kernels.cu (internal; plain C types only). */
+#ifndef PB_KERNELS_H
+#define PB_KERNELS_H
+
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#include "topology.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Largest CTA the labeling kernel is launched with (teams of up to 16 warps). */
+#define PB_CTA_THREADS 512
+
+#ifdef __CUDACC__
+typedef uint4 pb_u4;
+#else
+typedef struct { uint32_t x, y, z, w; } pb_u4;
+#endif
+
+/* Device view of one chunk_blocks' schedule. */
+typedef struct {
+    const pb_u4 *recs;       /* [S] packed node records, level order */
+    const pb_u4 *cv0;        /* [copies * S * 2] block-0 chaining values, or NULL */
+    const uint32_t *orank;   /* [S] local output rank, PB_NO_RANK otherwise */
+    const uint32_t *lstart;  /* [L + 1] */
+    uint32_t S, L, pool, half_w, retained;
+    uint32_t desc[8];        /* graph descriptor words */
+} pb_topo_view_t;
+
+/* One launch of the labeling kernel over `nunits` units of one topology:
+ * unit k is copy (k & (2^copies_log2 - 1)) of local chunk k >> copies_log2,
+ * whose seed is seeds[8*chunk..] and whose persisted super-chunk starts at
+ * persist + (first_super + chunk) * super_bytes. */
+typedef struct {
+    pb_topo_view_t topo;
+    const uint32_t *seeds;
+    uint8_t *persist;
+    uint64_t super_bytes;
+    uint64_t first_super;
+    uint8_t *scratch;            /* teams * team_scratch_bytes */
+    uint64_t team_scratch_bytes; /* G * pool * 32 */
+    uint32_t nunits;
+    uint32_t copies_log2;
+    uint32_t g_log2;             /* G = 2^g_log2 units per team */
+    uint32_t team_warps;         /* T warps per team */
+    uint32_t nbatches;           /* ceil(nunits / G) */
+    unsigned int *queue;         /* zeroed work counter */
+} pb_label_params_t;
+
+int pb_dev_set_keys(const uint32_t ksrc[8], const uint32_t kint[8], const uint32_t kseed[8]);
+int pb_dev_cv0_table(const void *recs, uint32_t S, uint32_t copies, void *cv0, cudaStream_t stream);
+int pb_dev_chunk_seeds(const uint8_t *d_session_seed, uint32_t seed_len, uint64_t rbo, uint32_t cb,
+                       uint32_t nchunks, uint64_t first_super, uint32_t *d_seeds,
+                       cudaStream_t stream);
+int pb_dev_label(const pb_label_params_t *params, uint32_t grid, uint32_t cta_threads,
+                 cudaStream_t stream);
+int pb_dev_label_occupancy(uint32_t cta_threads, int *blocks_per_sm);
+int pb_dev_label_single(uint32_t *d_out, int is_source, uint64_t node_index, const uint32_t *d_in,
+                        int have_p0, int have_p1, cudaStream_t stream);
+int pb_dev_compress_bench(uint32_t grid, uint32_t iters, uint32_t salt, uint32_t *d_sink,
+                          cudaStream_t stream);
+int pb_dev_compress_latency(uint32_t iters, unsigned long long *d_cycles, uint32_t *d_sink,
+                            cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,663 @@
+/*
+ * label_api.c — C11 host side of the B200 labeler: the drop-in C ABI of
+ * include/gpu_label.h and the additive ABI of include/pose_b200.h.
+ *
+ * Mirrors the reference host driver (common/src/cuda/label_gpu_common.cu and
+ * the warp strategy's label_gpu_run, common/src/cuda/label_gpu_warp.cu:
+ * 125-248) in behaviour: same entry points, same validation and return
+ * codes, synchronous calls, a topology bound to the device current at build
+ * time, scratch zeroed before the call returns.  The machinery differs:
+ *   - the schedule is this library's own (topology.c) and is uploaded once;
+ *   - per-chunk seeds are derived on the device (k_chunk_seeds) instead of a
+ *     host loop plus copy per batch;
+ *   - one persistent launch covers up to PB_MAX_CHUNKS_PER_LAUNCH chunks;
+ *     its schedule (team warps T, units per team G, resident teams) comes
+ *     from a throughput model over the topology's level widths;
+ *   - the scratch pool is kept on the topology across calls (grown on
+ *     demand) and zeroed at the end of every call and before it is freed.
+ */
+#include "b3_host.h"
+#include "kernels.h"
+#include "topology.h"
+
+#include "gpu_label.h"
+#include "pose_b200.h"
+
+#include <cuda_runtime_api.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#define PB_DEFAULT_CHUNK_BLOCKS 4096u
+#define PB_MAX_CHUNKS_PER_LAUNCH (1u << 20)
+#define PB_DEVICE_SEED_MAX 1016u /* seed_len + 8 must fit one BLAKE3 chunk */
+#define PB_SCRATCH_MARGIN ((uint64_t)2 << 30)
+
+static _Thread_local char g_err[512];
+
+static void set_err(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    fprintf(stderr, "%s\n", g_err);
+}
+
+const char *pose_b200_last_error(void) { return g_err; }
+
+static int quiet(void)
+{
+    const char *e = getenv("POSE_GPU_QUIET");
+    return (e && e[0] && e[0] != '0') ? 1 : 0;
+}
+
+static double now_sec(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+struct pose_hbm_topo {
+    int device;
+    uint32_t cb;
+    uint64_t super_bytes;
+    uint32_t copies;
+    uint32_t S, L, pool, half_w, retained, max_width;
+    uint8_t desc[32];
+    /* distinct level widths and how many levels have each (schedule model) */
+    uint32_t nw;
+    uint32_t *wval;
+    uint64_t *wcnt;
+    /* device schedule */
+    void *d_recs, *d_cv0, *d_orank, *d_lstart;
+    uint64_t dev_bytes;
+    pb_topo_view_t view;
+    /* per-topology workspace, reused across calls (one caller thread at a time) */
+    cudaStream_t stream;
+    cudaEvent_t ev[4];
+    uint8_t *d_scratch;
+    uint64_t scratch_alloc;
+    uint32_t *d_seeds;
+    uint64_t seeds_alloc; /* chunks */
+    uint8_t *d_sess;
+    size_t sess_alloc;
+    unsigned int *d_queue;
+    int occ256, occ512, sms;
+};
+
+/* ── schedule model ──────────────────────────────────────────────────────── */
+
+/* Model constants: integer lanes an SM retires per clock for this
+ * instruction mix, and the dependent latency of one node label in SM clocks.
+ * Defaults come from the compression microbenchmark; POSE_B200_INT_LANES and
+ * POSE_B200_LABEL_LATENCY override them. */
+static double model_lanes(void)
+{
+    const char *e = getenv("POSE_B200_INT_LANES");
+    double v = e ? atof(e) : 0.0;
+    return v > 0 ? v : 64.0;
+}
+
+static double model_latency(int cv0)
+{
+    const char *e = getenv("POSE_B200_LABEL_LATENCY");
+    double v = e ? atof(e) : 0.0;
+    return v > 0 ? v : (cv0 ? 1700.0 : 2300.0);
+}
+
+typedef struct {
+    uint32_t T, G, teams, grid, cta;
+    uint64_t team_scratch, scratch_bytes;
+    double cost;
+} plan_t;
+
+static uint64_t passes_for(const pose_hbm_topo_t *t, uint32_t T, uint32_t G)
+{
+    uint64_t lanes = 32ull * T, passes = 0;
+    for (uint32_t k = 0; k < t->nw; k++) {
+        uint64_t items = (uint64_t)G * t->wval[k];
+        passes += t->wcnt[k] * ((items + lanes - 1) / lanes);
+    }
+    return passes;
+}
+
+static int is_pow2(uint32_t v) { return v && !(v & (v - 1)); }
+
+static int make_plan(const pose_hbm_topo_t *t, uint64_t nunits, const pose_b200_sched_t *hint,
+                     uint64_t budget, plan_t *best)
+{
+    const double lanes_clk = model_lanes();
+    const double t_lat = model_latency(t->d_cv0 != NULL);
+    const double item_instr = t->d_cv0 ? 1400.0 : 2080.0;
+    memset(best, 0, sizeof(*best));
+    best->cost = -1;
+    for (uint32_t T = 1; T <= 16; T <<= 1) {
+        if (hint && hint->team_warps && hint->team_warps != T) continue;
+        uint32_t cta = T == 16 ? 512 : 256;
+        int occ = T == 16 ? t->occ512 : t->occ256;
+        if (occ <= 0) continue;
+        uint32_t tpc = cta / (32 * T);
+        for (uint32_t G = 1; G <= 32 && G <= 32 * T; G <<= 1) {
+            if (hint && hint->units_per_team && hint->units_per_team != G) continue;
+            uint64_t team_scratch = (uint64_t)G * t->pool * 32;
+            uint64_t batches = (nunits + G - 1) / G;
+            uint64_t cap = (uint64_t)t->sms * occ * tpc;
+            uint64_t memcap = team_scratch ? budget / team_scratch : cap;
+            uint64_t R = cap < memcap ? cap : memcap;
+            if (R > batches) R = batches;
+            if (hint && hint->max_teams && R > hint->max_teams) R = hint->max_teams;
+            if (R == 0) continue;
+            if (R > tpc && R < batches) R -= R % tpc; /* whole CTAs when capped */
+            uint64_t grid = (R + tpc - 1) / tpc;
+            uint64_t waves = (batches + R - 1) / R;
+            double items_sm = (double)R / t->sms * 32.0 * T;
+            double pass = items_sm * item_instr / lanes_clk;
+            if (pass < t_lat) pass = t_lat;
+            double cost = (double)waves * (double)passes_for(t, T, G) * pass;
+            uint64_t sbytes = grid * tpc * team_scratch;
+            if (sbytes > budget) continue;
+            if (best->cost < 0 || cost < best->cost * 0.999 ||
+                (cost <= best->cost * 1.001 && sbytes < best->scratch_bytes)) {
+                best->T = T; best->G = G; best->teams = (uint32_t)R;
+                best->grid = (uint32_t)grid; best->cta = cta;
+                best->team_scratch = team_scratch; best->scratch_bytes = sbytes;
+                best->cost = cost;
+            }
+        }
+    }
+    return best->cost < 0 ? -1 : 0;
+}
+
+/* ── helpers ─────────────────────────────────────────────────────────────── */
+
+#define CK(call, what)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            set_err("pose_b200: %s: CUDA error: %s", what, cudaGetErrorString(e_));      \
+            goto fail;                                                                   \
+        }                                                                                \
+    } while (0)
+
+static int grow(void **p, uint64_t *have, uint64_t need, size_t elem)
+{
+    if (*have >= need) return 0;
+    if (*p) cudaFree(*p);
+    *p = NULL;
+    *have = 0;
+    if (cudaMalloc(p, need * elem) != cudaSuccess) { *p = NULL; return -1; }
+    *have = need;
+    return 0;
+}
+
+static void free_workspace(pose_hbm_topo_t *t)
+{
+    if (t->d_scratch) {
+        cudaMemsetAsync(t->d_scratch, 0, t->scratch_alloc, t->stream);
+        cudaStreamSynchronize(t->stream);
+        cudaFree(t->d_scratch);
+    }
+    t->d_scratch = NULL;
+    t->scratch_alloc = 0;
+    if (t->d_seeds) {
+        cudaMemsetAsync(t->d_seeds, 0, t->seeds_alloc * 32, t->stream);
+        cudaStreamSynchronize(t->stream);
+        cudaFree(t->d_seeds);
+    }
+    t->d_seeds = NULL;
+    t->seeds_alloc = 0;
+    cudaFree(t->d_sess);
+    t->d_sess = NULL;
+    t->sess_alloc = 0;
+}
+
+/* ── build / free ────────────────────────────────────────────────────────── */
+
+void pose_graph_hbm_topo_free(pose_hbm_topo_t *t)
+{
+    if (!t) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != t->device) cudaSetDevice(t->device);
+    if (t->stream) free_workspace(t);
+    cudaFree(t->d_recs);
+    cudaFree(t->d_cv0);
+    cudaFree(t->d_orank);
+    cudaFree(t->d_lstart);
+    cudaFree(t->d_queue);
+    for (int i = 0; i < 4; i++) if (t->ev[i]) cudaEventDestroy(t->ev[i]);
+    if (t->stream) cudaStreamDestroy(t->stream);
+    if (prev >= 0 && prev != t->device) cudaSetDevice(prev);
+    free(t->wval);
+    free(t->wcnt);
+    free(t);
+}
+
+static int cmp_u32(const void *a, const void *b)
+{
+    uint32_t x = *(const uint32_t *)a, y = *(const uint32_t *)b;
+    return x < y ? -1 : x > y;
+}
+
+pose_hbm_topo_t *pose_b200_topo_build(uint32_t chunk_blocks, int with_cv0_table)
+{
+    uint32_t cb = chunk_blocks ? chunk_blocks : PB_DEFAULT_CHUNK_BLOCKS;
+    if (cb > PB_MAX_CHUNK_BLOCKS) {
+        set_err("pose_graph_hbm_topo_build: chunk_blocks %u out of range [1, %u]", cb,
+                PB_MAX_CHUNK_BLOCKS);
+        return NULL;
+    }
+    pb_topo_host_t h;
+    if (pb_topo_host_build(cb, &h) != 0) {
+        set_err("pose_graph_hbm_topo_build: schedule build failed for chunk_blocks %u", cb);
+        return NULL;
+    }
+    pose_hbm_topo_t *t = (pose_hbm_topo_t *)calloc(1, sizeof(*t));
+    uint32_t *ws = NULL;
+    if (!t) { set_err("pose_graph_hbm_topo_build: out of host memory"); goto fail_host; }
+    cudaGetDevice(&t->device);
+    t->cb = cb;
+    t->super_bytes = (uint64_t)cb * 32;
+    t->copies = h.retained ? 2 : 1;
+    t->S = h.S; t->L = h.L; t->pool = h.pool; t->half_w = h.half_w;
+    t->retained = h.retained; t->max_width = h.max_width;
+    memcpy(t->desc, h.desc, 32);
+
+    /* width histogram */
+    ws = (uint32_t *)malloc((size_t)h.L * 4);
+    if (!ws) { set_err("pose_graph_hbm_topo_build: out of host memory"); goto fail_host; }
+    for (uint32_t l = 0; l < h.L; l++) ws[l] = h.lstart[l + 1] - h.lstart[l];
+    qsort(ws, h.L, 4, cmp_u32);
+    t->wval = (uint32_t *)malloc((size_t)h.L * 4);
+    t->wcnt = (uint64_t *)malloc((size_t)h.L * 8);
+    if (!t->wval || !t->wcnt) { set_err("pose_graph_hbm_topo_build: out of host memory"); goto fail_host; }
+    for (uint32_t l = 0; l < h.L; l++) {
+        if (t->nw && t->wval[t->nw - 1] == ws[l]) t->wcnt[t->nw - 1]++;
+        else { t->wval[t->nw] = ws[l]; t->wcnt[t->nw] = 1; t->nw++; }
+    }
+    free(ws);
+    ws = NULL;
+
+    {
+        CK(cudaStreamCreate(&t->stream), "stream");
+        for (int i = 0; i < 4; i++) CK(cudaEventCreate(&t->ev[i]), "event");
+        CK(cudaMalloc(&t->d_recs, (size_t)h.S * 16), "topology records");
+        CK(cudaMalloc(&t->d_orank, (size_t)h.S * 4), "output ranks");
+        CK(cudaMalloc(&t->d_lstart, ((size_t)h.L + 1) * 4), "level offsets");
+        CK(cudaMalloc((void **)&t->d_queue, 64), "work counter");
+        t->dev_bytes = (uint64_t)h.S * 20 + ((uint64_t)h.L + 1) * 4;
+        CK(cudaMemcpyAsync(t->d_recs, h.recs, (size_t)h.S * 16, cudaMemcpyHostToDevice, t->stream),
+           "upload records");
+        CK(cudaMemcpyAsync(t->d_orank, h.orank, (size_t)h.S * 4, cudaMemcpyHostToDevice, t->stream),
+           "upload ranks");
+        CK(cudaMemcpyAsync(t->d_lstart, h.lstart, ((size_t)h.L + 1) * 4, cudaMemcpyHostToDevice,
+                           t->stream),
+           "upload levels");
+        uint32_t ksrc[8], kint[8], kseed[8];
+        pb_label_keys(ksrc, kint);
+        pb_context_key("pose-db/chunk-seed", kseed);
+        if (pb_dev_set_keys(ksrc, kint, kseed) != 0) {
+            set_err("pose_graph_hbm_topo_build: key upload failed");
+            goto fail;
+        }
+        if (with_cv0_table) {
+            uint64_t bytes = (uint64_t)t->copies * h.S * 32;
+            CK(cudaMalloc(&t->d_cv0, bytes), "block-0 table");
+            t->dev_bytes += bytes;
+            if (pb_dev_cv0_table(t->d_recs, h.S, t->copies, t->d_cv0, t->stream) != 0) {
+                set_err("pose_graph_hbm_topo_build: block-0 table kernel failed");
+                goto fail;
+            }
+        }
+        CK(cudaStreamSynchronize(t->stream), "build");
+        if (pb_dev_label_occupancy(256, &t->occ256) != 0 || pb_dev_label_occupancy(512, &t->occ512) != 0) {
+            set_err("pose_graph_hbm_topo_build: occupancy query failed");
+            goto fail;
+        }
+        CK(cudaDeviceGetAttribute(&t->sms, cudaDevAttrMultiProcessorCount, t->device), "SM count");
+        t->view.recs = (const pb_u4 *)t->d_recs;
+        t->view.cv0 = (const pb_u4 *)t->d_cv0;
+        t->view.orank = (const uint32_t *)t->d_orank;
+        t->view.lstart = (const uint32_t *)t->d_lstart;
+        t->view.S = h.S; t->view.L = h.L; t->view.pool = h.pool;
+        t->view.half_w = h.half_w; t->view.retained = h.retained;
+        for (int i = 0; i < 8; i++)
+            t->view.desc[i] = (uint32_t)h.desc[4 * i] | ((uint32_t)h.desc[4 * i + 1] << 8) |
+                              ((uint32_t)h.desc[4 * i + 2] << 16) | ((uint32_t)h.desc[4 * i + 3] << 24);
+    }
+    pb_topo_host_free(&h);
+    return t;
+
+fail:
+    pb_topo_host_free(&h);
+    pose_graph_hbm_topo_free(t);
+    return NULL;
+fail_host:
+    free(ws);
+    pb_topo_host_free(&h);
+    if (t) { free(t->wval); free(t->wcnt); free(t); }
+    return NULL;
+}
+
+pose_hbm_topo_t *pose_graph_hbm_topo_build(uint32_t chunk_blocks, pose_hash_algo_t algo)
+{
+    if (algo != POSE_HASH_BLAKE3) {
+        set_err("pose_graph_hbm_topo_build: only BLAKE3 supported on GPU");
+        return NULL;
+    }
+    return pose_b200_topo_build(chunk_blocks, 1);
+}
+
+void pose_b200_topo_info(const pose_hbm_topo_t *t, uint32_t *chunk_blocks, uint64_t *nodes_per_chunk,
+                         uint32_t *levels, uint32_t *pool_slots, uint64_t *device_bytes)
+{
+    if (!t) return;
+    if (chunk_blocks) *chunk_blocks = t->cb;
+    if (nodes_per_chunk) *nodes_per_chunk = 2ull * t->S;
+    if (levels) *levels = t->L;
+    if (pool_slots) *pool_slots = t->pool;
+    if (device_bytes) *device_bytes = t->dev_bytes;
+}
+
+/* ── labeling ────────────────────────────────────────────────────────────── */
+
+static uint64_t scratch_budget(const pose_hbm_topo_t *t, const pose_b200_sched_t *s)
+{
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    uint64_t avail = (uint64_t)fr + t->scratch_alloc;
+    avail = avail > PB_SCRATCH_MARGIN ? avail - PB_SCRATCH_MARGIN : avail / 2;
+    if (s && s->scratch_cap_bytes && s->scratch_cap_bytes < avail) avail = s->scratch_cap_bytes;
+    return avail;
+}
+
+int pose_b200_plan(const pose_hbm_topo_t *t, uint64_t super_chunks, const pose_b200_sched_t *hint,
+                   pose_b200_sched_t *out)
+{
+    if (!t || !out) return -1;
+    uint64_t chunks = super_chunks < PB_MAX_CHUNKS_PER_LAUNCH ? super_chunks : PB_MAX_CHUNKS_PER_LAUNCH;
+    plan_t p;
+    if (chunks == 0 || make_plan(t, chunks * t->copies, hint, scratch_budget(t, hint), &p) != 0)
+        return -1;
+    memset(out, 0, sizeof(*out));
+    out->team_warps = p.T;
+    out->units_per_team = p.G;
+    out->max_teams = p.teams;
+    out->scratch_cap_bytes = p.scratch_bytes;
+    return 0;
+}
+
+int pose_b200_topo_label(const pose_hbm_topo_t *ct, const uint8_t *session_seed, size_t seed_len,
+                         void *hbm_dev_ptr, size_t hbm_len, uint64_t rbo,
+                         const pose_b200_sched_t *sched, pose_b200_stats_t *stats)
+{
+    pose_hbm_topo_t *t = (pose_hbm_topo_t *)ct; /* workspace is mutable state */
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (!t) { set_err("pose_graph_hbm_topo_label: NULL topology"); return -1; }
+    uint64_t num_super = hbm_len / t->super_bytes;
+    if (num_super == 0) return 0; /* smaller than one super-chunk: nothing to label */
+    if (!hbm_dev_ptr) { set_err("pose_graph_hbm_topo_label: NULL buffer"); return -1; }
+    if (!session_seed && seed_len) { set_err("pose_graph_hbm_topo_label: NULL seed"); return -1; }
+    if (sched && ((sched->team_warps && (!is_pow2(sched->team_warps) || sched->team_warps > 16)) ||
+                  (sched->units_per_team &&
+                   (!is_pow2(sched->units_per_team) || sched->units_per_team > 32)))) {
+        set_err("pose_b200_topo_label: schedule must use powers of two (T <= 16, G <= 32)");
+        return -1;
+    }
+    int prev = -1, rc = -1;
+    uint32_t *h_seeds = NULL;
+    cudaGetDevice(&prev);
+    if (prev != t->device && cudaSetDevice(t->device) != cudaSuccess) {
+        set_err("pose_graph_hbm_topo_label: cannot select the topology's device");
+        return -1;
+    }
+
+    const uint64_t per_launch = num_super < PB_MAX_CHUNKS_PER_LAUNCH ? num_super : PB_MAX_CHUNKS_PER_LAUNCH;
+    plan_t plan;
+    if (make_plan(t, per_launch * t->copies, sched, scratch_budget(t, sched), &plan) != 0) {
+        set_err("pose_graph_hbm_topo_label: no schedule fits the scratch budget "
+                "(one copy needs %llu bytes)", (unsigned long long)t->pool * 32ull);
+        goto out;
+    }
+    if (!quiet()) {
+        printf("  GPU label: strategy=b200  %llu super-chunks  scaffold=%llu nodes  "
+               "T=%u G=%u teams=%u\n",
+               (unsigned long long)num_super, 2ull * t->S, plan.T, plan.G, plan.teams);
+        fflush(stdout);
+    }
+    {
+        double t0 = now_sec();
+        if (grow((void **)&t->d_scratch, &t->scratch_alloc, plan.scratch_bytes, 1) != 0) {
+            set_err("pose_graph_hbm_topo_label: scratch alloc of %llu bytes failed",
+                    (unsigned long long)plan.scratch_bytes);
+            goto out;
+        }
+        if (grow((void **)&t->d_seeds, &t->seeds_alloc, per_launch, 32) != 0) {
+            set_err("pose_graph_hbm_topo_label: seed buffer alloc failed");
+            goto out;
+        }
+        const int dev_seeds = seed_len <= PB_DEVICE_SEED_MAX;
+        if (dev_seeds && seed_len) {
+            uint64_t have = t->sess_alloc;
+            if (grow((void **)&t->d_sess, &have, seed_len, 1) != 0) {
+                set_err("pose_graph_hbm_topo_label: seed alloc failed");
+                goto out;
+            }
+            t->sess_alloc = (size_t)have;
+            CK(cudaMemcpyAsync(t->d_sess, session_seed, seed_len, cudaMemcpyHostToDevice, t->stream),
+               "seed upload");
+        }
+        CK(cudaEventRecord(t->ev[0], t->stream), "event");
+        float kms = 0;
+        uint32_t launches = 0;
+        for (uint64_t first = 0; first < num_super; first += per_launch) {
+            uint64_t n = num_super - first < per_launch ? num_super - first : per_launch;
+            if (dev_seeds) {
+                if (pb_dev_chunk_seeds(t->d_sess, (uint32_t)seed_len, rbo, t->cb, (uint32_t)n, first,
+                                       t->d_seeds, t->stream) != 0) {
+                    set_err("pose_graph_hbm_topo_label: chunk-seed kernel failed");
+                    goto out;
+                }
+            } else {
+                /* long session seeds: derive on the host */
+                if (!h_seeds) h_seeds = (uint32_t *)malloc(per_launch * 32);
+                if (!h_seeds) { set_err("pose_graph_hbm_topo_label: out of host memory"); goto out; }
+                for (uint64_t j = 0; j < n; j++) {
+                    uint8_t cs[32];
+                    pb_chunk_seed(cs, session_seed, seed_len, (rbo + (first + j) * (uint64_t)t->cb) / t->cb);
+                    memcpy(h_seeds + 8 * j, cs, 32);
+                }
+                CK(cudaMemcpyAsync(t->d_seeds, h_seeds, n * 32, cudaMemcpyHostToDevice, t->stream),
+                   "seed upload");
+                CK(cudaStreamSynchronize(t->stream), "seed upload");
+            }
+            CK(cudaMemsetAsync(t->d_queue, 0, 64, t->stream), "queue reset");
+            pb_label_params_t p;
+            memset(&p, 0, sizeof(p));
+            p.topo = t->view;
+            p.seeds = t->d_seeds;
+            p.persist = (uint8_t *)hbm_dev_ptr;
+            p.super_bytes = t->super_bytes;
+            p.first_super = first;
+            p.scratch = t->d_scratch;
+            p.team_scratch_bytes = plan.team_scratch;
+            p.nunits = (uint32_t)(n * t->copies);
+            p.copies_log2 = t->copies == 2 ? 1 : 0;
+            p.g_log2 = (uint32_t)__builtin_ctz(plan.G);
+            p.team_warps = plan.T;
+            p.nbatches = (uint32_t)((p.nunits + plan.G - 1) / plan.G);
+            p.queue = t->d_queue;
+            CK(cudaEventRecord(t->ev[1], t->stream), "event");
+            if (pb_dev_label(&p, plan.grid, plan.cta, t->stream) != 0) {
+                set_err("pose_graph_hbm_topo_label: label kernel launch failed: %s",
+                        cudaGetErrorString(cudaGetLastError()));
+                goto out;
+            }
+            CK(cudaEventRecord(t->ev[2], t->stream), "event");
+            launches++;
+            CK(cudaEventSynchronize(t->ev[2]), "label kernel");
+            float ms = 0;
+            cudaEventElapsedTime(&ms, t->ev[1], t->ev[2]);
+            kms += ms;
+        }
+        /* scratch and seeds never outlive the call (the reference zeroes its
+         * scratch before freeing it, label_gpu_warp.cu:236-238) */
+        CK(cudaMemsetAsync(t->d_scratch, 0, plan.scratch_bytes, t->stream), "scratch zero");
+        CK(cudaMemsetAsync(t->d_seeds, 0, per_launch * 32, t->stream), "seed zero");
+        CK(cudaEventRecord(t->ev[3], t->stream), "event");
+        CK(cudaStreamSynchronize(t->stream), "label");
+        float tms = 0;
+        cudaEventElapsedTime(&tms, t->ev[0], t->ev[3]);
+        double elapsed = now_sec() - t0;
+        if (stats) {
+            stats->kernel_ms = kms;
+            stats->total_ms = tms;
+            stats->super_chunks = num_super;
+            stats->units = num_super * t->copies;
+            stats->nodes = num_super * t->copies * (uint64_t)t->S;
+            stats->scratch_bytes = plan.scratch_bytes;
+            stats->team_warps = plan.T;
+            stats->units_per_team = plan.G;
+            stats->teams = plan.teams;
+            stats->kernel_launches = launches;
+            stats->used_cv0_table = t->d_cv0 != NULL;
+        }
+        if (!quiet() && elapsed > 0) {
+            double mib = (double)(num_super * t->super_bytes) / (double)(1u << 20);
+            printf("  GPU wipe: %.0f MiB in %.3f s = %.1f MiB/s\n", mib, elapsed, mib / elapsed);
+            fflush(stdout);
+        }
+        rc = 0;
+    }
+fail:
+out:
+    free(h_seeds);
+    if (rc != 0) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) fprintf(stderr, "pose_graph_hbm_topo_label: CUDA error: %s\n", cudaGetErrorString(e));
+    }
+    if (prev >= 0 && prev != t->device) cudaSetDevice(prev);
+    return rc;
+}
+
+int pose_graph_hbm_topo_label(const pose_hbm_topo_t *topo, const uint8_t *session_seed,
+                              size_t seed_len, void *hbm_dev_ptr, size_t hbm_len,
+                              uint64_t region_block_offset)
+{
+    return pose_b200_topo_label(topo, session_seed, seed_len, hbm_dev_ptr, hbm_len,
+                                region_block_offset, NULL, NULL);
+}
+
+int pose_graph_label_hbm(const uint8_t *session_seed, size_t seed_len, uint32_t chunk_blocks,
+                         void *hbm_dev_ptr, size_t hbm_len, uint64_t region_block_offset,
+                         pose_hash_algo_t algo)
+{
+    if (algo != POSE_HASH_BLAKE3) {
+        set_err("pose_graph_label_hbm: only BLAKE3 supported on GPU");
+        return -1;
+    }
+    uint32_t cb = chunk_blocks ? chunk_blocks : PB_DEFAULT_CHUNK_BLOCKS;
+    if (cb > PB_MAX_CHUNK_BLOCKS) {
+        set_err("pose_graph_label_hbm: super_blocks out of range");
+        return -1;
+    }
+    if (hbm_len / ((size_t)cb * 32) == 0) return 0;
+    pose_hbm_topo_t *t = pose_graph_hbm_topo_build(cb, algo);
+    if (!t) return -1;
+    int rc = pose_graph_hbm_topo_label(t, session_seed, seed_len, hbm_dev_ptr, hbm_len,
+                                       region_block_offset);
+    pose_graph_hbm_topo_free(t);
+    return rc;
+}
+
+/* ── known-answer helper ─────────────────────────────────────────────────── */
+
+static void le_words(uint32_t *w, const uint8_t *p)
+{
+    for (int i = 0; i < 8; i++)
+        w[i] = (uint32_t)p[4 * i] | ((uint32_t)p[4 * i + 1] << 8) | ((uint32_t)p[4 * i + 2] << 16) |
+               ((uint32_t)p[4 * i + 3] << 24);
+}
+
+int pose_gpu_label_node_single(uint8_t out[32], int is_source, uint64_t node_index,
+                               const uint8_t *pred0, const uint8_t *pred1, const uint8_t *seed,
+                               const uint8_t *descriptor, const uint32_t key_src[8],
+                               const uint32_t key_int[8])
+{
+    if (!out || !seed || !descriptor || !key_src || !key_int) {
+        set_err("pose_gpu_label_node_single: NULL argument");
+        return -1;
+    }
+    uint32_t in[56];
+    memset(in, 0, sizeof(in));
+    if (pred0) le_words(in, pred0);
+    if (pred1) le_words(in + 8, pred1);
+    le_words(in + 16, seed);
+    le_words(in + 24, descriptor);
+    memcpy(in + 32, key_src, 32);
+    memcpy(in + 40, key_int, 32);
+    uint32_t *d = NULL, res[8];
+    int rc = -1;
+    CK(cudaMalloc((void **)&d, sizeof(in)), "KAT alloc");
+    CK(cudaMemcpy(d, in, sizeof(in), cudaMemcpyHostToDevice), "KAT upload");
+    if (pb_dev_label_single(d + 48, is_source, node_index, d, pred0 != NULL, pred1 != NULL, 0) != 0) {
+        set_err("pose_gpu_label_node_single: launch failed");
+        goto fail;
+    }
+    CK(cudaDeviceSynchronize(), "KAT kernel");
+    CK(cudaMemcpy(res, d + 48, 32, cudaMemcpyDeviceToHost), "KAT download");
+    for (int i = 0; i < 8; i++) {
+        out[4 * i] = (uint8_t)res[i];
+        out[4 * i + 1] = (uint8_t)(res[i] >> 8);
+        out[4 * i + 2] = (uint8_t)(res[i] >> 16);
+        out[4 * i + 3] = (uint8_t)(res[i] >> 24);
+    }
+    rc = 0;
+fail:
+    cudaFree(d);
+    return rc;
+}
+
+/* ── compression-rate microbenchmark ─────────────────────────────────────── */
+
+double pose_b200_compress_rate(uint32_t iters, double *latency_cycles)
+{
+    int dev = 0, sms = 0;
+    uint32_t *d_sink = NULL;
+    unsigned long long *d_cyc = NULL, cyc = 0;
+    cudaEvent_t a = NULL, b = NULL;
+    double rate = 0;
+    cudaGetDevice(&dev);
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    CK(cudaMalloc((void **)&d_sink, 4096 * 4), "sink");
+    CK(cudaMalloc((void **)&d_cyc, 8), "cycles");
+    CK(cudaEventCreate(&a), "event");
+    CK(cudaEventCreate(&b), "event");
+    {
+        uint32_t grid = (uint32_t)sms * 8; /* 8 CTAs x 256 threads per SM */
+        if (pb_dev_compress_bench(grid, iters / 8 + 1, 1, d_sink, 0) != 0) goto fail; /* warm-up */
+        CK(cudaEventRecord(a, 0), "event");
+        if (pb_dev_compress_bench(grid, iters, 2, d_sink, 0) != 0) goto fail;
+        CK(cudaEventRecord(b, 0), "event");
+        CK(cudaEventSynchronize(b), "bench");
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        rate = (double)grid * 256.0 * iters / (ms * 1e-3);
+        if (latency_cycles) {
+            if (pb_dev_compress_latency(iters, d_cyc, d_sink, 0) != 0) goto fail;
+            CK(cudaMemcpy(&cyc, d_cyc, 8, cudaMemcpyDeviceToHost), "cycles");
+            *latency_cycles = (double)cyc / iters;
+        }
+    }
+fail:
+    cudaFree(d_sink);
+    cudaFree(d_cyc);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    return rate;
+}

@@ -1,0 +1,140 @@
+"""GPU parity: every label the B200 path persists must be byte-identical to
+the reference CPU path on the same seed and positions.
+
+Oracles: the golden fixtures made by the reference compiled from source
+(tests/golden/), and the C restatement in oracle/ for randomised cases.
+All calls go through the C ABI (libpose_b200.so)."""
+from __future__ import annotations
+
+import hashlib
+import random
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def dev_buffer(torch, nbytes: int, fill: int = 0xA5):
+    return torch.full((max(1, nbytes),), fill, dtype=torch.uint8, device="cuda")
+
+
+def host_bytes(t) -> bytes:
+    return t.cpu().numpy().tobytes()
+
+
+def label_region(pkg, torch, key, cb, nsuper, rbo, sched=None, cv0=True, extra=0):
+    buf = dev_buffer(torch, nsuper * cb * 32 + extra)
+    with pkg.Topology(cb, cv0_table=cv0) as topo:
+        rc = topo.label(key, buf.data_ptr(), nsuper * cb * 32 + extra, rbo, sched=sched)
+    torch.cuda.synchronize()
+    assert rc == 0, pkg.last_error()
+    return host_bytes(buf)
+
+
+def test_kat_single_node(pkg, cuda, oracle):
+    k = golden("hash_kats.json")
+    for c in k["labels"]:
+        p0 = bytes.fromhex(c["p0"]) if c["p0"] else None
+        p1 = bytes.fromhex(c["p1"]) if c["p1"] else None
+        got = pkg.label_node_single(c["is_source"], c["index"], p0, p1, bytes.fromhex(c["seed"]),
+                                    bytes.fromhex(c["desc"]), k["key_src"], k["key_int"])
+        assert got is not None and got.hex() == c["hex"]
+    rnd = random.Random(7)
+    for _ in range(16):
+        idx = rnd.randrange(1 << 64)
+        p0 = rnd.randbytes(32)
+        seed, desc = rnd.randbytes(32), rnd.randbytes(32)
+        got = pkg.label_node_single(0, idx, p0, None, seed, desc, k["key_src"], k["key_int"])
+        assert got == oracle.label_node(0, idx, p0, None, seed, desc)
+
+
+def test_small_regions_all_bytes(pkg, cuda):
+    for r in golden("small_regions.json"):
+        key = bytes.fromhex(r["key"])
+        for cv0 in (True, False):
+            got = label_region(pkg, cuda, key, r["chunk_blocks"], r["super_chunks"], r["rbo"], cv0=cv0)
+            assert got.hex() == r["hex"], (r["chunk_blocks"], r["rbo"], cv0)
+
+
+def test_plain_small_config(pkg, cuda, wl):
+    g = golden("configs.json")["plain_small"]
+    c = wl.plain_small()
+    got = label_region(pkg, cuda, c["key"], c["chunk_blocks"], c["chunks"], c["rbo"])
+    sb = c["chunk_blocks"] * 32
+    for j in range(c["chunks"]):
+        assert hashlib.sha256(got[j * sb:(j + 1) * sb]).hexdigest() == g["super_chunk_sha256"][j], j
+    assert hashlib.sha256(got).hexdigest() == g["region_sha256"]
+
+
+@pytest.mark.parametrize("T,G", [(1, 1), (1, 2), (1, 4), (1, 8), (1, 32), (2, 1), (4, 4), (8, 2), (16, 1), (16, 32)])
+def test_every_schedule_gives_the_same_bytes(pkg, cuda, wl, T, G):
+    g = golden("configs.json")["plain_small"]
+    c = wl.plain_small()
+    s = pkg.Sched(team_warps=T, units_per_team=G)
+    got = label_region(pkg, cuda, c["key"], c["chunk_blocks"], c["chunks"], c["rbo"], sched=s,
+                       cv0=(G % 2 == 0))
+    assert hashlib.sha256(got).hexdigest() == g["region_sha256"]
+
+
+def test_few_resident_teams_loop_over_the_queue(pkg, cuda, wl):
+    # 128 units through 3 resident teams: every team pulls many batches
+    g = golden("configs.json")["plain_small"]
+    c = wl.plain_small()
+    s = pkg.Sched(team_warps=1, units_per_team=2, max_teams=3)
+    got = label_region(pkg, cuda, c["key"], c["chunk_blocks"], c["chunks"], c["rbo"], sched=s)
+    assert hashlib.sha256(got).hexdigest() == g["region_sha256"]
+
+
+def test_random_regions_vs_oracle(pkg, cuda, oracle):
+    rnd = random.Random(11)
+    for _ in range(12):
+        cb = rnd.choice([1, 2, 3, 6, 8, 33, 64, 255, 256, 1000, 2048])
+        nsup = rnd.randint(1, 9)
+        rbo = rnd.choice([0, rnd.randrange(1 << 40), cb * rnd.randrange(1 << 20)])
+        key = rnd.randbytes(rnd.choice([32, 0, 7, 64]))
+        got = label_region(pkg, cuda, key, cb, nsup, rbo)
+        want = oracle.label_region(key, cb, nsup, rbo, threads=8).tobytes()
+        assert got == want, (cb, nsup, rbo, len(key))
+
+
+def test_tail_and_short_buffers_are_untouched(pkg, cuda, oracle):
+    key = b"\x11" * 32
+    cb, nsup, extra = 16, 3, 16 * 32 - 32
+    got = label_region(pkg, cuda, key, cb, nsup, 5, extra=extra)
+    assert got[: nsup * cb * 32] == oracle.label_region(key, cb, nsup, 5).tobytes()
+    assert got[nsup * cb * 32:] == b"\xa5" * extra
+    buf = dev_buffer(cuda, cb * 32)
+    with pkg.Topology(cb) as topo:
+        assert topo.label(key, buf.data_ptr(), cb * 32 - 1, 0) == 0
+    assert host_bytes(buf) == b"\xa5" * (cb * 32)
+
+
+def test_one_shot_entry_point_and_defaults(pkg, cuda, oracle):
+    key = b"\x22" * 32
+    buf = dev_buffer(cuda, 2 * 4096 * 32)
+    assert pkg.label_hbm(key, 0, buf.data_ptr(), 2 * 4096 * 32, 4096) == 0  # 0 -> 4096
+    cuda.cuda.synchronize()
+    assert host_bytes(buf) == oracle.label_region(key, 4096, 2, 4096, threads=2).tobytes()
+    assert pkg.label_hbm(key, 16, buf.data_ptr(), 64, 0, pkg.POSE_HASH_SHA256) == -1
+
+
+def test_topology_reused_across_calls_and_seeds(pkg, cuda, oracle):
+    with pkg.Topology(100) as topo:
+        for i in range(3):
+            key = bytes([i]) * 32
+            buf = dev_buffer(cuda, 4 * 100 * 32)
+            assert topo.label(key, buf.data_ptr(), 4 * 100 * 32, 100 * i) == 0
+            assert host_bytes(buf) == oracle.label_region(key, 100, 4, 100 * i, threads=4).tobytes()
+
+
+def test_stats_report_the_work(pkg, cuda):
+    buf = dev_buffer(cuda, 8 * 1024 * 32)
+    with pkg.Topology(1024) as topo:
+        rc, st = topo.label(b"s" * 32, buf.data_ptr(), 8 * 1024 * 32, 0, stats=True)
+    assert rc == 0
+    assert st["super_chunks"] == 8 and st["units"] == 16
+    assert st["nodes"] == 8 * 96254
+    assert st["kernel_ms"] > 0 and st["kernel_launches"] == 1

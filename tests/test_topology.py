@@ -1,0 +1,187 @@
+"""The product's host-side schedule (csrc/topology.c) and host BLAKE3
+(csrc/b3_host.c), built without CUDA as _build/libpose_b200_host.so.
+
+Checks: the copy edges reproduce the reference's pose_graph_edges numbering
+(via the golden digests), and the recycled slot map is safe for level-parallel
+labelling — recomputed independently here the way the reference's own
+test_slot_map.c checks live ranges (common/test/test_slot_map.c:50-135).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import hashlib
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import PKG_DIR, golden
+
+u8p = C.POINTER(C.c_uint8)
+u32p = C.POINTER(C.c_uint32)
+
+
+class HostTopo(C.Structure):
+    _fields_ = [("cb", C.c_uint32), ("n", C.c_int), ("half_w", C.c_uint32),
+                ("retained", C.c_uint32), ("S", C.c_uint32), ("L", C.c_uint32),
+                ("pool", C.c_uint32), ("max_width", C.c_uint32), ("lstart", u32p),
+                ("recs", u32p), ("orank", u32p), ("desc", C.c_uint8 * 32)]
+
+
+@pytest.fixture(scope="module")
+def host():
+    path = os.path.join(PKG_DIR, "_build", "libpose_b200_host.so")
+    if not os.path.exists(path):
+        subprocess.run(["make", "-s", "-C", PKG_DIR, "host"], check=True)
+    L = C.CDLL(path)
+    L.pb_copy_node_count.argtypes = [C.c_uint32]
+    L.pb_copy_node_count.restype = C.c_uint64
+    L.pb_chunk_node_count.argtypes = [C.c_uint32]
+    L.pb_chunk_node_count.restype = C.c_uint64
+    L.pb_topo_copy_edges.argtypes = [C.c_uint32, u8p, u32p, u32p, u32p]
+    L.pb_topo_copy_edges.restype = C.c_uint64
+    L.pb_topo_host_build.argtypes = [C.c_uint32, C.POINTER(HostTopo)]
+    L.pb_topo_host_build.restype = C.c_int
+    L.pb_topo_host_free.argtypes = [C.POINTER(HostTopo)]
+    L.pb_chunk_seed.argtypes = [u8p, u8p, C.c_size_t, C.c_uint64]
+    L.pb_graph_descriptor.argtypes = [u8p, C.c_uint64, C.c_uint64]
+    L.pb_label_keys.argtypes = [u32p, u32p]
+    L.pb_parameter_n.argtypes = [C.c_uint64]
+    L.pb_parameter_n.restype = C.c_int
+    return L
+
+
+def copy_edges(L, cb):
+    S = L.pb_copy_node_count(cb)
+    np_ = np.zeros(S, np.uint8)
+    p0 = np.zeros(S, np.uint32)
+    p1 = np.zeros(S, np.uint32)
+    n = L.pb_parameter_n(cb)
+    outs = np.zeros(1 << n, np.uint32)
+    assert L.pb_topo_copy_edges(cb, np_.ctypes.data_as(u8p), p0.ctypes.data_as(u32p),
+                                p1.ctypes.data_as(u32p), outs.ctypes.data_as(u32p)) == S
+    return np_, p0, p1, outs
+
+
+def chunk_edges(L, cb):
+    """Assemble the whole chunk (left copy, right copy shifted by S) in the
+    reference's pose_graph_edges format."""
+    np_, p0, p1, outs = copy_edges(L, cb)
+    S = len(np_)
+    n = L.pb_parameter_n(cb)
+    hw = 1 << n
+    ret = cb - hw
+    rp0 = np.concatenate([p0, np.where(np_ >= 1, p0 + S, 0).astype(np.uint32)])
+    rp1 = np.concatenate([p1, np.where(np_ == 2, p1 + S, 0).astype(np.uint32)])
+    rank = np.full(2 * S, -1, np.int32)
+    rank[outs] = np.arange(hw, dtype=np.int32)
+    rank[outs[:ret].astype(np.int64) + S] = hw + np.arange(ret, dtype=np.int32)
+    return np.concatenate([np_, np_]), rp0, rp1, rank
+
+
+def test_chunk_edges_match_reference(host):
+    for e in golden("edges.json"):
+        np_, p0, p1, rk = chunk_edges(host, e["m"])
+        assert len(np_) == e["count"] == host.pb_chunk_node_count(e["m"])
+        assert hashlib.sha256(np_.tobytes()).hexdigest() == e["np"], e["m"]
+        assert hashlib.sha256(p0.tobytes()).hexdigest() == e["p0"], e["m"]
+        assert hashlib.sha256(p1.tobytes()).hexdigest() == e["p1"], e["m"]
+        assert hashlib.sha256(rk.tobytes()).hexdigest() == e["rank"], e["m"]
+
+
+def test_host_b3_matches_reference(host):
+    k = golden("hash_kats.json")
+    a = np.zeros(8, np.uint32)
+    b = np.zeros(8, np.uint32)
+    host.pb_label_keys(a.ctypes.data_as(u32p), b.ctypes.data_as(u32p))
+    assert a.tolist() == k["key_src"] and b.tolist() == k["key_int"]
+    for d in k["descriptors"]:
+        out = (C.c_uint8 * 32)()
+        host.pb_graph_descriptor(C.cast(out, u8p), d["m"], d["n"])
+        assert bytes(out).hex() == d["hex"]
+        assert host.pb_parameter_n(d["m"]) == d["n"]
+    for c in k["chunk_seeds"]:
+        seed = bytes.fromhex(c["seed"])
+        out = (C.c_uint8 * 32)()
+        sbuf = (C.c_uint8 * max(1, len(seed))).from_buffer_copy(seed or b"\0")
+        host.pb_chunk_seed(C.cast(out, u8p), C.cast(sbuf, u8p), len(seed), c["index"])
+        assert bytes(out).hex() == c["hex"], (len(seed), c["index"])
+
+
+def schedule(L, cb):
+    t = HostTopo()
+    assert L.pb_topo_host_build(cb, C.byref(t)) == 0
+    lstart = np.ctypeslib.as_array(t.lstart, shape=(t.L + 1,)).copy()
+    recs = np.ctypeslib.as_array(t.recs, shape=(t.S, 4)).copy()
+    orank = np.ctypeslib.as_array(t.orank, shape=(t.S,)).copy()
+    info = {k: getattr(t, k) for k in ("cb", "n", "half_w", "retained", "S", "L", "pool", "max_width")}
+    desc = bytes(t.desc)
+    L.pb_topo_host_free(C.byref(t))
+    return info, lstart, recs, orank, desc
+
+
+@pytest.mark.parametrize("cb", [1, 2, 3, 5, 16, 17, 100, 1024, 4096])
+def test_schedule_is_level_parallel_safe(host, cb):
+    info, lstart, recs, orank, desc = schedule(host, cb)
+    np_, p0, p1, outs = copy_edges(host, cb)
+    S, L, pool = info["S"], info["L"], info["pool"]
+    ids = (recs[:, 0] & 0x0FFFFFFF).astype(np.int64)
+    npr = (recs[:, 0] >> 28) & 3
+    outbit = (recs[:, 0] >> 30) & 1
+    # the records are a permutation of the copy's nodes, ordered by level
+    assert sorted(ids.tolist()) == list(range(S))
+    assert (npr == np_[ids]).all()
+    assert outbit.sum() == info["half_w"]
+    r = orank[outbit == 1]
+    assert sorted(r.tolist()) == list(range(info["half_w"]))
+    assert (orank[outbit == 0] == 0xFFFFFFFF).all()
+    assert (outs[r] == ids[outbit == 1]).all()
+    level = np.zeros(S, np.int64)
+    for l in range(L):
+        level[ids[lstart[l]:lstart[l + 1]]] = l
+    # levels are dependency levels: 1 + max(level(pred))
+    want = np.zeros(S, np.int64)
+    for i in range(S):
+        if np_[i] >= 1:
+            want[i] = level[p0[i]] + 1
+        if np_[i] == 2:
+            want[i] = max(want[i], level[p1[i]] + 1)
+    assert (want == level).all()
+    # slot safety, simulated level by level: every predecessor read in a level
+    # sees its own label, and no slot is written twice within a level nor
+    # written while it is read in that level
+    slot_of = np.full(S, -1, np.int64)
+    content = np.full(pool, -1, np.int64)
+    assert recs[:, 3].max() < pool and recs[:, 1].max() < pool and recs[:, 2].max() < pool
+    for l in range(L):
+        seg = recs[lstart[l]:lstart[l + 1]]
+        sid = ids[lstart[l]:lstart[l + 1]]
+        for k in range(len(seg)):
+            i = sid[k]
+            if np_[i] >= 1:
+                assert seg[k, 1] == slot_of[p0[i]] and content[seg[k, 1]] == p0[i]
+            if np_[i] == 2:
+                assert seg[k, 2] == slot_of[p1[i]] and content[seg[k, 2]] == p1[i]
+        dst = seg[:, 3].astype(np.int64)
+        assert len(set(dst.tolist())) == len(dst)
+        reads = set(seg[npr[lstart[l]:lstart[l + 1]] >= 1, 1].tolist()) | \
+            set(seg[npr[lstart[l]:lstart[l + 1]] == 2, 2].tolist())
+        assert not (reads & set(dst.tolist()))
+        content[dst] = sid
+        slot_of[sid] = dst
+    assert pool <= 8 * (1 << info["n"])
+
+
+def test_schedule_sizes(host):
+    info, lstart, recs, orank, desc = schedule(host, 1 << 17)
+    assert info["S"] == 18087935 and 2 * info["S"] == 36175870
+    assert info["L"] == 393197
+    assert info["pool"] <= 2 * (1 << 16) * 2
+    assert lstart[-1] == info["S"]
+
+
+def test_bad_chunk_blocks(host):
+    t = HostTopo()
+    assert host.pb_topo_host_build(0, C.byref(t)) == -1
+    assert host.pb_topo_host_build((1 << 20) + 1, C.byref(t)) == -1
