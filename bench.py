@@ -56,6 +56,12 @@ def workload(name: str) -> dict:
     elif name == "window_2e17":
         # the reference's default 16 GiB HBM window at 2^17 (4096 super-chunks)
         w = dict(wl.plain_2e17(), name="window_2e17", chunks=4096)
+    elif name == "throughput_2e12":
+        # profiling case: many chunks in flight, ~0.1 s kernel, scratch + store > L2
+        w = dict(wl.plain_2e17(), name="throughput_2e12", chunk_blocks=1 << 12, chunks=2048)
+    elif name == "latency_2e14":
+        # profiling case: few chunks, depth-bound, ~0.1 s kernel
+        w = dict(wl.plain_2e17(), name="latency_2e14", chunk_blocks=1 << 14, chunks=16)
     else:
         raise SystemExit(f"unknown workload {name}")
     w["nodes_per_chunk"] = wl.chunk_nodes(w["chunk_blocks"])

@@ -23,7 +23,7 @@ typedef struct {
     uint32_t team_warps;        /* T: warps that cooperate on one batch (1..16, power of 2) */
     uint32_t units_per_team;    /* G: chunk copies run in lockstep by one team (1..32, power of 2) */
     uint32_t max_teams;         /* cap on resident teams (0 = occupancy and memory bound) */
-    uint32_t reserved;
+    uint32_t kernel;            /* 0 = automatic, 1 = basic lockstep kernel, 2 = pipelined kernel */
     uint64_t scratch_cap_bytes; /* cap on the scratch pool (0 = free HBM less a margin) */
 } pose_b200_sched_t;
 
@@ -37,7 +37,7 @@ typedef struct {
     uint64_t scratch_bytes;     /* scratch pool bytes used */
     uint32_t team_warps, units_per_team, teams, kernel_launches;
     uint32_t used_cv0_table;    /* 1 when block 0 came from the precomputed table */
-    uint32_t reserved;
+    uint32_t kernel;            /* 1 = basic lockstep kernel, 2 = pipelined kernel */
 } pose_b200_stats_t;
 
 /* Extends pose_graph_hbm_topo_build (common/include/gpu_label.h:77-78).

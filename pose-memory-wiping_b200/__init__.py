@@ -36,7 +36,7 @@ class Sched(C.Structure):
     """pose_b200_sched_t: zero fields mean automatic."""
 
     _fields_ = [("team_warps", C.c_uint32), ("units_per_team", C.c_uint32),
-                ("max_teams", C.c_uint32), ("reserved", C.c_uint32),
+                ("max_teams", C.c_uint32), ("kernel", C.c_uint32),
                 ("scratch_cap_bytes", C.c_uint64)]
 
 
@@ -48,10 +48,10 @@ class Stats(C.Structure):
                 ("scratch_bytes", C.c_uint64), ("team_warps", C.c_uint32),
                 ("units_per_team", C.c_uint32), ("teams", C.c_uint32),
                 ("kernel_launches", C.c_uint32), ("used_cv0_table", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("kernel", C.c_uint32)]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 _u8p = C.POINTER(C.c_uint8)

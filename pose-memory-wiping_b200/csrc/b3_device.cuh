@@ -65,6 +65,46 @@ __device__ __forceinline__ void g_mix(uint32_t &a, uint32_t &b, uint32_t &c, uin
     b = rotr7(b ^ c);
 }
 
+/* The same G with its additions issued as integer multiply-adds by a
+ * run-time 1 (`one`, opaque to the compiler): they then execute on the FMA
+ * pipe instead of the integer ALU pipe, which otherwise carries all twelve
+ * operations of G (adds, xors, funnel shifts and byte permutes) and bounds
+ * throughput when every SM is full.  a + b + m becomes two multiply-adds
+ * (b*1 + m, then a*1 + that), so the dependent chain is longer: use it where
+ * throughput, not latency, is the limit. */
+__device__ __forceinline__ uint32_t madd(uint32_t a, uint32_t one, uint32_t b)
+{
+    uint32_t r;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(one), "r"(b));
+    return r;
+}
+
+__device__ __forceinline__ void g_mix_fma(uint32_t &a, uint32_t &b, uint32_t &c, uint32_t &d,
+                                          uint32_t x, uint32_t y, uint32_t one)
+{
+    a = madd(a, one, madd(b, one, x));
+    d = rotr16(d ^ a);
+    c = madd(c, one, d);
+    b = rotr12(b ^ c);
+    a = madd(a, one, madd(b, one, y));
+    d = rotr8(d ^ a);
+    c = madd(c, one, d);
+    b = rotr7(b ^ c);
+}
+
+template <int R>
+__device__ __forceinline__ void round_fma(uint32_t (&v)[16], const uint32_t (&m)[16], uint32_t one)
+{
+    g_mix_fma(v[0], v[4], v[8], v[12], m[sched(R, 0)], m[sched(R, 1)], one);
+    g_mix_fma(v[1], v[5], v[9], v[13], m[sched(R, 2)], m[sched(R, 3)], one);
+    g_mix_fma(v[2], v[6], v[10], v[14], m[sched(R, 4)], m[sched(R, 5)], one);
+    g_mix_fma(v[3], v[7], v[11], v[15], m[sched(R, 6)], m[sched(R, 7)], one);
+    g_mix_fma(v[0], v[5], v[10], v[15], m[sched(R, 8)], m[sched(R, 9)], one);
+    g_mix_fma(v[1], v[6], v[11], v[12], m[sched(R, 10)], m[sched(R, 11)], one);
+    g_mix_fma(v[2], v[7], v[8], v[13], m[sched(R, 12)], m[sched(R, 13)], one);
+    g_mix_fma(v[3], v[4], v[9], v[14], m[sched(R, 14)], m[sched(R, 15)], one);
+}
+
 template <int R>
 __device__ __forceinline__ void round_fn(uint32_t (&v)[16], const uint32_t (&m)[16])
 {
@@ -92,6 +132,23 @@ __device__ __forceinline__ void compress(uint32_t (&cv)[8], const uint32_t (&m)[
     round_fn<4>(v, m);
     round_fn<5>(v, m);
     round_fn<6>(v, m);
+#pragma unroll
+    for (int i = 0; i < 8; i++) cv[i] = v[i] ^ v[i + 8];
+}
+
+/* compress() with the FMA-pipe additions of g_mix_fma (same result). */
+__device__ __forceinline__ void compress_fma(uint32_t (&cv)[8], const uint32_t (&m)[16],
+                                             uint32_t block_len, uint32_t flags, uint32_t one)
+{
+    uint32_t v[16] = {cv[0], cv[1], cv[2], cv[3], cv[4], cv[5], cv[6], cv[7],
+                      kIV0,  kIV1,  kIV2,  kIV3,  0u,    0u,    block_len, flags};
+    round_fma<0>(v, m, one);
+    round_fma<1>(v, m, one);
+    round_fma<2>(v, m, one);
+    round_fma<3>(v, m, one);
+    round_fma<4>(v, m, one);
+    round_fma<5>(v, m, one);
+    round_fma<6>(v, m, one);
 #pragma unroll
     for (int i = 0; i < 8; i++) cv[i] = v[i] ^ v[i + 8];
 }

@@ -49,7 +49,45 @@ typedef struct {
     uint32_t team_warps;         /* T warps per team */
     uint32_t nbatches;           /* ceil(nunits / G) */
     unsigned int *queue;         /* zeroed work counter */
+    uint32_t fma_adds;           /* 1: additions on the FMA pipe (throughput-bound launches) */
+    uint32_t one;                /* must be 1 */
 } pb_label_params_t;
+
+/* Device view of the pipelined records (topology.h, PB_REF_*). */
+typedef struct {
+    const pb_u4 *recs2;      /* [2 * S] pipelined records, level order */
+    const pb_u4 *cv0;        /* [copies * S * 2] block-0 chaining values (required) */
+    const uint32_t *lstart;  /* [L + 1] */
+    uint32_t S, L, half_w, retained;
+    uint32_t csm;            /* shared-memory label slots per chunk copy */
+    uint32_t gpool;          /* global label slots per chunk copy */
+    uint32_t desc[8];
+} pb_topo_view2_t;
+
+/* One launch of the pipelined kernel; fields as in pb_label_params_t.  The
+ * dynamic shared memory holds teams_per_cta * csm * G labels followed by the
+ * staging area (12 x 16 bytes per thread). */
+typedef struct {
+    pb_topo_view2_t topo;
+    const uint32_t *seeds;
+    uint8_t *persist;
+    uint64_t super_bytes;
+    uint64_t first_super;
+    uint8_t *scratch;
+    uint64_t team_scratch_bytes; /* G * gpool * 32 */
+    uint32_t nunits;
+    uint32_t copies_log2;
+    uint32_t g_log2;
+    uint32_t team_warps;
+    uint32_t nbatches;
+    unsigned int *queue;
+} pb_pipe_params_t;
+
+#define PB_PIPE_STAGE_BYTES_PER_THREAD 192u
+
+int pb_dev_label_pipe(const pb_pipe_params_t *params, uint32_t grid, uint32_t cta_threads,
+                      uint32_t smem_bytes, cudaStream_t stream);
+int pb_dev_label_pipe_occupancy(uint32_t cta_threads, uint32_t smem_bytes, int *blocks_per_sm);
 
 int pb_dev_set_keys(const uint32_t ksrc[8], const uint32_t kint[8], const uint32_t kseed[8]);
 int pb_dev_cv0_table(const void *recs, uint32_t S, uint32_t copies, void *cv0, cudaStream_t stream);
@@ -62,7 +100,7 @@ int pb_dev_label_occupancy(uint32_t cta_threads, int *blocks_per_sm);
 int pb_dev_label_single(uint32_t *d_out, int is_source, uint64_t node_index, const uint32_t *d_in,
                         int have_p0, int have_p1, cudaStream_t stream);
 int pb_dev_compress_bench(uint32_t grid, uint32_t iters, uint32_t salt, uint32_t *d_sink,
-                          cudaStream_t stream);
+                          int fma_adds, cudaStream_t stream);
 int pb_dev_compress_latency(uint32_t iters, unsigned long long *d_cycles, uint32_t *d_sink,
                             cudaStream_t stream);
 

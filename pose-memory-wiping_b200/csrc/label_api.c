@@ -74,9 +74,11 @@ struct pose_hbm_topo {
     uint32_t *wval;
     uint64_t *wcnt;
     /* device schedule */
-    void *d_recs, *d_cv0, *d_orank, *d_lstart;
+    void *d_recs, *d_cv0, *d_orank, *d_lstart, *d_recs2;
     uint64_t dev_bytes;
     pb_topo_view_t view;
+    pb_topo_view2_t view2; /* pipelined records (d_recs2 != NULL) */
+    int occ_pipe[5][2];    /* pipelined kernel CTAs/SM for T = 1..16, G = 1, 2 (-1 = not queried) */
     /* per-topology workspace, reused across calls (one caller thread at a time) */
     cudaStream_t stream;
     cudaEvent_t ev[4];
@@ -100,21 +102,48 @@ static double model_lanes(void)
 {
     const char *e = getenv("POSE_B200_INT_LANES");
     double v = e ? atof(e) : 0.0;
-    return v > 0 ? v : 64.0;
+    return v > 0 ? v : 72.0;
 }
 
 static double model_latency(int cv0)
 {
     const char *e = getenv("POSE_B200_LABEL_LATENCY");
     double v = e ? atof(e) : 0.0;
-    return v > 0 ? v : (cv0 ? 1700.0 : 2300.0);
+    return v > 0 ? v : (cv0 ? 6000.0 : 7000.0);
+}
+
+static double model_pipe_latency(void)
+{
+    const char *e = getenv("POSE_B200_PIPE_LATENCY");
+    double v = e ? atof(e) : 0.0;
+    return v > 0 ? v : 2800.0;
 }
 
 typedef struct {
-    uint32_t T, G, teams, grid, cta;
+    uint32_t T, G, teams, grid, cta, kernel, smem, fma;
     uint64_t team_scratch, scratch_bytes;
     double cost;
 } plan_t;
+
+#define PB_CSM_LATENCY 2048u /* shared-memory label slots per copy in the pipelined records */
+
+static uint32_t pipe_smem_bytes(const pose_hbm_topo_t *t, uint32_t T, uint32_t G)
+{
+    return t->view2.csm * G * 32u + 32u * T * PB_PIPE_STAGE_BYTES_PER_THREAD;
+}
+
+static int pipe_occupancy(pose_hbm_topo_t *t, uint32_t T, uint32_t G)
+{
+    int ti = __builtin_ctz(T), gi = G == 1 ? 0 : 1;
+    if (t->occ_pipe[ti][gi] < 0) {
+        int occ = 0;
+        uint32_t smem = pipe_smem_bytes(t, T, G);
+        if (smem > 227u * 1024u || pb_dev_label_pipe_occupancy(32 * T, smem, &occ) != 0) occ = 0;
+        cudaGetLastError();
+        t->occ_pipe[ti][gi] = occ;
+    }
+    return t->occ_pipe[ti][gi];
+}
 
 static uint64_t passes_for(const pose_hbm_topo_t *t, uint32_t T, uint32_t G)
 {
@@ -128,45 +157,64 @@ static uint64_t passes_for(const pose_hbm_topo_t *t, uint32_t T, uint32_t G)
 
 static int is_pow2(uint32_t v) { return v && !(v & (v - 1)); }
 
-static int make_plan(const pose_hbm_topo_t *t, uint64_t nunits, const pose_b200_sched_t *hint,
+/* Throughput model of one launch.  A team's batch takes at least its
+ * latency-bound time (every pass of every level waits for a label: t_lat per
+ * pass for the basic kernel; the pipelined kernel's first pass of a level
+ * costs t_pipe, further passes t_lat), and an SM needs at least its ALU time
+ * (all node hashes of the teams resident on it at lanes_clk lane-operations
+ * per clock).  A launch runs ceil(batches / resident teams) waves of the
+ * larger of the two. */
+static int make_plan(const pose_hbm_topo_t *ct, uint64_t nunits, const pose_b200_sched_t *hint,
                      uint64_t budget, plan_t *best)
 {
+    pose_hbm_topo_t *t = (pose_hbm_topo_t *)ct; /* occupancy cache */
     const double lanes_clk = model_lanes();
     const double t_lat = model_latency(t->d_cv0 != NULL);
+    const double t_pipe = model_pipe_latency();
     const double item_instr = t->d_cv0 ? 1400.0 : 2080.0;
+    const int want = hint ? (int)hint->kernel : 0;
     memset(best, 0, sizeof(*best));
     best->cost = -1;
-    for (uint32_t T = 1; T <= 16; T <<= 1) {
-        if (hint && hint->team_warps && hint->team_warps != T) continue;
-        uint32_t cta = T == 16 ? 512 : 256;
-        int occ = T == 16 ? t->occ512 : t->occ256;
-        if (occ <= 0) continue;
-        uint32_t tpc = cta / (32 * T);
-        for (uint32_t G = 1; G <= 32 && G <= 32 * T; G <<= 1) {
-            if (hint && hint->units_per_team && hint->units_per_team != G) continue;
-            uint64_t team_scratch = (uint64_t)G * t->pool * 32;
-            uint64_t batches = (nunits + G - 1) / G;
-            uint64_t cap = (uint64_t)t->sms * occ * tpc;
-            uint64_t memcap = team_scratch ? budget / team_scratch : cap;
-            uint64_t R = cap < memcap ? cap : memcap;
-            if (R > batches) R = batches;
-            if (hint && hint->max_teams && R > hint->max_teams) R = hint->max_teams;
-            if (R == 0) continue;
-            if (R > tpc && R < batches) R -= R % tpc; /* whole CTAs when capped */
-            uint64_t grid = (R + tpc - 1) / tpc;
-            uint64_t waves = (batches + R - 1) / R;
-            double items_sm = (double)R / t->sms * 32.0 * T;
-            double pass = items_sm * item_instr / lanes_clk;
-            if (pass < t_lat) pass = t_lat;
-            double cost = (double)waves * (double)passes_for(t, T, G) * pass;
-            uint64_t sbytes = grid * tpc * team_scratch;
-            if (sbytes > budget) continue;
-            if (best->cost < 0 || cost < best->cost * 0.999 ||
-                (cost <= best->cost * 1.001 && sbytes < best->scratch_bytes)) {
-                best->T = T; best->G = G; best->teams = (uint32_t)R;
-                best->grid = (uint32_t)grid; best->cta = cta;
-                best->team_scratch = team_scratch; best->scratch_bytes = sbytes;
-                best->cost = cost;
+    for (int kernel = 1; kernel <= 2; kernel++) {
+        if (want && want != kernel) continue;
+        if (kernel == 2 && !t->d_recs2) continue;
+        for (uint32_t T = kernel == 2 ? 4 : 1; T <= 16; T <<= 1) {
+            if (hint && hint->team_warps && hint->team_warps != T) continue;
+            uint32_t cta = kernel == 2 ? 32 * T : (T == 16 ? 512 : 256);
+            uint32_t tpc = cta / (32 * T);
+            for (uint32_t G = 1; G <= 32 && G <= 32 * T && (kernel == 1 || G <= 2); G <<= 1) {
+                if (hint && hint->units_per_team && hint->units_per_team != G) continue;
+                int occ = kernel == 2 ? pipe_occupancy(t, T, G) : (T == 16 ? t->occ512 : t->occ256);
+                if (occ <= 0) continue;
+                uint64_t slots = kernel == 2 ? (t->view2.gpool ? t->view2.gpool : 1) : t->pool;
+                uint64_t team_scratch = (uint64_t)G * slots * 32;
+                uint64_t batches = (nunits + G - 1) / G;
+                uint64_t cap = (uint64_t)t->sms * occ * tpc;
+                uint64_t memcap = budget / team_scratch;
+                uint64_t R = cap < memcap ? cap : memcap;
+                if (R > batches) R = batches;
+                if (hint && hint->max_teams && R > hint->max_teams) R = hint->max_teams;
+                if (R == 0) continue;
+                if (R > tpc && R < batches) R -= R % tpc; /* whole CTAs when capped */
+                uint64_t grid = (R + tpc - 1) / tpc;
+                uint64_t sbytes = grid * tpc * team_scratch;
+                if (sbytes > budget) continue;
+                uint64_t waves = (batches + R - 1) / R;
+                uint64_t passes = passes_for(t, T, G);
+                double lat = kernel == 2 ? (double)t->L * t_pipe + (double)(passes - t->L) * t_lat
+                                         : (double)passes * t_lat;
+                double teams_sm = (double)((R + t->sms - 1) / t->sms);
+                double alu = teams_sm * G * (double)t->S * item_instr / lanes_clk;
+                double cost = (double)waves * (lat > alu ? lat : alu);
+                if (best->cost < 0 || cost < best->cost * 0.999 ||
+                    (cost <= best->cost * 1.001 && sbytes < best->scratch_bytes)) {
+                    best->T = T; best->G = G; best->teams = (uint32_t)R;
+                    best->grid = (uint32_t)grid; best->cta = cta;
+                    best->team_scratch = team_scratch; best->scratch_bytes = sbytes;
+                    best->cost = cost; best->kernel = (uint32_t)kernel;
+                    best->smem = kernel == 2 ? pipe_smem_bytes(t, T, G) : 0;
+                    best->fma = kernel == 1 && alu >= lat; /* ALU-bound: move adds to the FMA pipe */
+                }
             }
         }
     }
@@ -226,6 +274,7 @@ void pose_graph_hbm_topo_free(pose_hbm_topo_t *t)
     if (prev != t->device) cudaSetDevice(t->device);
     if (t->stream) free_workspace(t);
     cudaFree(t->d_recs);
+    cudaFree(t->d_recs2);
     cudaFree(t->d_cv0);
     cudaFree(t->d_orank);
     cudaFree(t->d_lstart);
@@ -253,7 +302,7 @@ pose_hbm_topo_t *pose_b200_topo_build(uint32_t chunk_blocks, int with_cv0_table)
         return NULL;
     }
     pb_topo_host_t h;
-    if (pb_topo_host_build(cb, &h) != 0) {
+    if (pb_topo_host_build_ex(cb, with_cv0_table ? PB_CSM_LATENCY : 0, &h) != 0) {
         set_err("pose_graph_hbm_topo_build: schedule build failed for chunk_blocks %u", cb);
         return NULL;
     }
@@ -305,6 +354,12 @@ pose_hbm_topo_t *pose_b200_topo_build(uint32_t chunk_blocks, int with_cv0_table)
             set_err("pose_graph_hbm_topo_build: key upload failed");
             goto fail;
         }
+        if (with_cv0_table && h.recs2) {
+            CK(cudaMalloc(&t->d_recs2, (size_t)h.S * 32), "pipelined records");
+            CK(cudaMemcpyAsync(t->d_recs2, h.recs2, (size_t)h.S * 32, cudaMemcpyHostToDevice, t->stream),
+               "upload pipelined records");
+            t->dev_bytes += (uint64_t)h.S * 32;
+        }
         if (with_cv0_table) {
             uint64_t bytes = (uint64_t)t->copies * h.S * 32;
             CK(cudaMalloc(&t->d_cv0, bytes), "block-0 table");
@@ -329,6 +384,13 @@ pose_hbm_topo_t *pose_b200_topo_build(uint32_t chunk_blocks, int with_cv0_table)
         for (int i = 0; i < 8; i++)
             t->view.desc[i] = (uint32_t)h.desc[4 * i] | ((uint32_t)h.desc[4 * i + 1] << 8) |
                               ((uint32_t)h.desc[4 * i + 2] << 16) | ((uint32_t)h.desc[4 * i + 3] << 24);
+        t->view2.recs2 = (const pb_u4 *)t->d_recs2;
+        t->view2.cv0 = (const pb_u4 *)t->d_cv0;
+        t->view2.lstart = (const uint32_t *)t->d_lstart;
+        t->view2.S = h.S; t->view2.L = h.L; t->view2.half_w = h.half_w;
+        t->view2.retained = h.retained; t->view2.csm = h.csm; t->view2.gpool = h.gpool2;
+        memcpy(t->view2.desc, t->view.desc, sizeof(t->view2.desc));
+        memset(t->occ_pipe, 0xFF, sizeof(t->occ_pipe));
     }
     pb_topo_host_free(&h);
     return t;
@@ -388,6 +450,7 @@ int pose_b200_plan(const pose_hbm_topo_t *t, uint64_t super_chunks, const pose_b
     out->team_warps = p.T;
     out->units_per_team = p.G;
     out->max_teams = p.teams;
+    out->kernel = p.kernel;
     out->scratch_cap_bytes = p.scratch_bytes;
     return 0;
 }
@@ -407,6 +470,10 @@ int pose_b200_topo_label(const pose_hbm_topo_t *ct, const uint8_t *session_seed,
                   (sched->units_per_team &&
                    (!is_pow2(sched->units_per_team) || sched->units_per_team > 32)))) {
         set_err("pose_b200_topo_label: schedule must use powers of two (T <= 16, G <= 32)");
+        return -1;
+    }
+    if (sched && sched->kernel > 2) {
+        set_err("pose_b200_topo_label: kernel must be 0 (automatic), 1 or 2");
         return -1;
     }
     int prev = -1, rc = -1;
@@ -492,8 +559,25 @@ int pose_b200_topo_label(const pose_hbm_topo_t *ct, const uint8_t *session_seed,
             p.team_warps = plan.T;
             p.nbatches = (uint32_t)((p.nunits + plan.G - 1) / plan.G);
             p.queue = t->d_queue;
+            p.fma_adds = plan.fma;
+            p.one = 1;
+            { const char *e = getenv("POSE_B200_FMA_ADDS"); if (e && e[0]) p.fma_adds = (uint32_t)atoi(e); }
             CK(cudaEventRecord(t->ev[1], t->stream), "event");
-            if (pb_dev_label(&p, plan.grid, plan.cta, t->stream) != 0) {
+            int lrc;
+            if (plan.kernel == 2) {
+                pb_pipe_params_t pp;
+                memset(&pp, 0, sizeof(pp));
+                pp.topo = t->view2;
+                pp.seeds = p.seeds; pp.persist = p.persist; pp.super_bytes = p.super_bytes;
+                pp.first_super = p.first_super; pp.scratch = p.scratch;
+                pp.team_scratch_bytes = plan.team_scratch; pp.nunits = p.nunits;
+                pp.copies_log2 = p.copies_log2; pp.g_log2 = p.g_log2; pp.team_warps = p.team_warps;
+                pp.nbatches = p.nbatches; pp.queue = p.queue;
+                lrc = pb_dev_label_pipe(&pp, plan.grid, plan.cta, plan.smem, t->stream);
+            } else {
+                lrc = pb_dev_label(&p, plan.grid, plan.cta, t->stream);
+            }
+            if (lrc != 0) {
                 set_err("pose_graph_hbm_topo_label: label kernel launch failed: %s",
                         cudaGetErrorString(cudaGetLastError()));
                 goto out;
@@ -526,6 +610,7 @@ int pose_b200_topo_label(const pose_hbm_topo_t *ct, const uint8_t *session_seed,
             stats->teams = plan.teams;
             stats->kernel_launches = launches;
             stats->used_cv0_table = t->d_cv0 != NULL;
+            stats->kernel = plan.kernel;
         }
         if (!quiet() && elapsed > 0) {
             double mib = (double)(num_super * t->super_bytes) / (double)(1u << 20);
@@ -640,14 +725,17 @@ double pose_b200_compress_rate(uint32_t iters, double *latency_cycles)
     CK(cudaEventCreate(&b), "event");
     {
         uint32_t grid = (uint32_t)sms * 8; /* 8 CTAs x 256 threads per SM */
-        if (pb_dev_compress_bench(grid, iters / 8 + 1, 1, d_sink, 0) != 0) goto fail; /* warm-up */
-        CK(cudaEventRecord(a, 0), "event");
-        if (pb_dev_compress_bench(grid, iters, 2, d_sink, 0) != 0) goto fail;
-        CK(cudaEventRecord(b, 0), "event");
-        CK(cudaEventSynchronize(b), "bench");
-        float ms = 0;
-        cudaEventElapsedTime(&ms, a, b);
-        rate = (double)grid * 256.0 * iters / (ms * 1e-3);
+        for (int fma = 0; fma <= 1; fma++) {
+            if (pb_dev_compress_bench(grid, iters / 8 + 1, 1, d_sink, fma, 0) != 0) goto fail; /* warm-up */
+            CK(cudaEventRecord(a, 0), "event");
+            if (pb_dev_compress_bench(grid, iters, 2, d_sink, fma, 0) != 0) goto fail;
+            CK(cudaEventRecord(b, 0), "event");
+            CK(cudaEventSynchronize(b), "bench");
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            double r = (double)grid * 256.0 * iters / (ms * 1e-3);
+            if (r > rate) rate = r;
+        }
         if (latency_cycles) {
             if (pb_dev_compress_latency(iters, d_cyc, d_sink, 0) != 0) goto fail;
             CK(cudaMemcpy(&cyc, d_cyc, 8, cudaMemcpyDeviceToHost), "cycles");

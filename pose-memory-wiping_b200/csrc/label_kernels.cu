@@ -121,6 +121,7 @@ __global__ void __launch_bounds__(128) k_chunk_seeds(const uint8_t *__restrict__
 
 /* ── the labeling kernel ─────────────────────────────────────────────────── */
 
+template <bool FMA>
 __global__ void __launch_bounds__(PB_CTA_THREADS) k_label(const __grid_constant__ pb_label_params_t p)
 {
     const uint32_t T = p.team_warps;
@@ -204,13 +205,19 @@ __global__ void __launch_bounds__(PB_CTA_THREADS) k_label(const __grid_constant_
                         uint32_t m0[16];
                         key_words(cv, np == 0);
                         block0_words(m0, (rec.x & PB_REC_ID_MASK) + id_off);
-                        compress(cv, m0, 64, kFlagsBlock0);
+                        if (FMA) compress_fma(cv, m0, 64, kFlagsBlock0, p.one);
+                        else compress(cv, m0, 64, kFlagsBlock0);
                     }
-                    compress(cv, m, 64, kFlagsBlock1);
                     uint32_t m2[16];
 #pragma unroll
                     for (int i = 0; i < 8; i++) { m2[i] = seed[i]; m2[8 + i] = tp.desc[i]; }
-                    compress(cv, m2, 64, kFlagsBlock2);
+                    if (FMA) {
+                        compress_fma(cv, m, 64, kFlagsBlock1, p.one);
+                        compress_fma(cv, m2, 64, kFlagsBlock2, p.one);
+                    } else {
+                        compress(cv, m, 64, kFlagsBlock1);
+                        compress(cv, m2, 64, kFlagsBlock2);
+                    }
                     const uint4 o0 = make_uint4(cv[0], cv[1], cv[2], cv[3]);
                     const uint4 o1 = make_uint4(cv[4], cv[5], cv[6], cv[7]);
                     uint4 *d = tscr + (((size_t)rec.w << glog) + u) * 2;
@@ -265,8 +272,9 @@ __global__ void k_label_single(uint32_t *out, int is_source, uint64_t node_index
  * work cannot be elided.  Counting compressions / time with every SM full
  * gives the sustained compression rate of this GPU for the exact instruction
  * mix the labeler issues. */
+template <bool FMA>
 __global__ void __launch_bounds__(256) k_compress_bench(uint32_t iters, uint32_t salt,
-                                                        uint32_t *sink)
+                                                        uint32_t *sink, uint32_t one)
 {
     uint32_t cv[8], m[16];
 #pragma unroll
@@ -274,7 +282,8 @@ __global__ void __launch_bounds__(256) k_compress_bench(uint32_t iters, uint32_t
 #pragma unroll
     for (int i = 0; i < 16; i++) m[i] = blockIdx.x * 0x85EBCA6Bu + i * 0x27D4EB2Fu;
     for (uint32_t k = 0; k < iters; k++) {
-        compress(cv, m, 64, kFlagsBlock1);
+        if (FMA) compress_fma(cv, m, 64, kFlagsBlock1, one);
+        else compress(cv, m, 64, kFlagsBlock1);
 #pragma unroll
         for (int i = 0; i < 8; i++) m[i] ^= cv[i];
     }
@@ -345,16 +354,19 @@ extern "C" int pb_dev_chunk_seeds(const uint8_t *d_session_seed, uint32_t seed_l
 extern "C" int pb_dev_label(const pb_label_params_t *params, uint32_t grid, uint32_t cta_threads,
                             cudaStream_t stream)
 {
-    pb::k_label<<<grid, cta_threads, 0, stream>>>(*params);
+    if (params->fma_adds) pb::k_label<true><<<grid, cta_threads, 0, stream>>>(*params);
+    else pb::k_label<false><<<grid, cta_threads, 0, stream>>>(*params);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int pb_dev_label_occupancy(uint32_t cta_threads, int *blocks_per_sm)
 {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pb::k_label,
-                                                         (int)cta_threads, 0) == cudaSuccess
-               ? 0
-               : -1;
+    int a = 0, b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, pb::k_label<false>, (int)cta_threads, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, pb::k_label<true>, (int)cta_threads, 0) != cudaSuccess)
+        return -1;
+    *blocks_per_sm = a < b ? a : b;
+    return 0;
 }
 
 extern "C" int pb_dev_label_single(uint32_t *d_out, int is_source, uint64_t node_index,
@@ -366,9 +378,10 @@ extern "C" int pb_dev_label_single(uint32_t *d_out, int is_source, uint64_t node
 }
 
 extern "C" int pb_dev_compress_bench(uint32_t grid, uint32_t iters, uint32_t salt, uint32_t *d_sink,
-                                     cudaStream_t stream)
+                                     int fma_adds, cudaStream_t stream)
 {
-    pb::k_compress_bench<<<grid, 256, 0, stream>>>(iters, salt, d_sink);
+    if (fma_adds) pb::k_compress_bench<true><<<grid, 256, 0, stream>>>(iters, salt, d_sink, 1u);
+    else pb::k_compress_bench<false><<<grid, 256, 0, stream>>>(iters, salt, d_sink, 1u);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -183,10 +183,87 @@ void pb_topo_host_free(pb_topo_host_t *t)
     free(t->lstart);
     free(t->recs);
     free(t->orank);
+    free(t->recs2);
     memset(t, 0, sizeof(*t));
 }
 
-int pb_topo_host_build(uint32_t cb, pb_topo_host_t *t)
+/* Pipelined records: every node read at its next level gets a shared-memory
+ * copy (while the pool has room); a global slot is kept only for nodes read
+ * two or more levels later or left without a shared-memory copy.  Both pools
+ * are assigned greedily level by level, allocation before release, so two
+ * labels that are live in the same level never share a slot. */
+static int build_pipelined(uint32_t S, uint32_t L, const uint8_t *np, const uint32_t *p0,
+                           const uint32_t *p1, const uint32_t *lvl, const uint32_t *dies,
+                           const uint32_t *order, const uint32_t *lstart, const uint32_t *cntd,
+                           const uint32_t *dorder, const uint32_t *rank_of, uint32_t csm,
+                           pb_topo_host_t *t)
+{
+    uint8_t *d1 = (uint8_t *)calloc(S, 1);
+    uint32_t *ss = (uint32_t *)malloc((size_t)S * 4), *gs = (uint32_t *)malloc((size_t)S * 4);
+    uint32_t *gstack = (uint32_t *)malloc((size_t)S * 4);
+    uint32_t *sstack = (uint32_t *)malloc(((size_t)csm + 1) * 4);
+    uint32_t *recs = (uint32_t *)malloc((size_t)S * 32);
+    int rc = -1;
+    if (!d1 || !ss || !gs || !gstack || !sstack || !recs) goto out;
+    for (uint32_t id = 0; id < S; id++) {
+        if (np[id] >= 1 && lvl[p0[id]] + 1 == lvl[id]) d1[p0[id]] = 1;
+        if (np[id] >= 2 && lvl[p1[id]] + 1 == lvl[id]) d1[p1[id]] = 1;
+    }
+    uint32_t gtop = 0, gfresh = 0, stop = 0, sfresh = 0;
+    for (uint32_t l = 0; l < L; l++) {
+        for (uint32_t p = lstart[l]; p < lstart[l + 1]; p++) {
+            uint32_t id = order[p];
+            ss[id] = PB_NO_SLOT;
+            if (d1[id]) {
+                if (stop) ss[id] = sstack[--stop];
+                else if (sfresh < csm) ss[id] = sfresh++;
+            }
+        }
+        for (uint32_t p = lstart[l]; p < lstart[l + 1]; p++) {
+            uint32_t id = order[p];
+            int need_g = dies[id] >= lvl[id] + 2 || (d1[id] && ss[id] == PB_NO_SLOT);
+            gs[id] = need_g ? (gtop ? gstack[--gtop] : gfresh++) : PB_NO_SLOT;
+        }
+        for (uint32_t k = cntd[l]; k < cntd[l + 1]; k++) {
+            uint32_t id = dorder[k];
+            if (gs[id] != PB_NO_SLOT) gstack[gtop++] = gs[id];
+        }
+        if (l > 0)
+            for (uint32_t p = lstart[l - 1]; p < lstart[l]; p++)
+                if (ss[order[p]] != PB_NO_SLOT) sstack[stop++] = ss[order[p]];
+    }
+    for (uint32_t p = 0; p < S; p++) {
+        uint32_t id = order[p], k = np[id], *r = recs + (size_t)8 * p;
+        uint32_t ref[2] = {0, 0};
+        for (uint32_t e = 0; e < k; e++) {
+            uint32_t q = e == 0 ? p0[id] : p1[id];
+            if (lvl[q] + 1 == lvl[id])
+                ref[e] = PB_REF_PREV | (ss[q] != PB_NO_SLOT ? (PB_REF_SMEM | ss[q]) : gs[q]);
+            else
+                ref[e] = gs[q];
+        }
+        r[0] = id | (k << PB_REC_NP_SHIFT) | (rank_of[id] != PB_NO_RANK ? PB_REC_OUT_BIT : 0);
+        r[1] = ref[0];
+        r[2] = ref[1];
+        r[3] = gs[id];
+        r[4] = ss[id];
+        r[5] = rank_of[id];
+        r[6] = 0;
+        r[7] = 0;
+    }
+    t->recs2 = recs;
+    recs = NULL;
+    t->csm = sfresh;
+    t->gpool2 = gfresh;
+    rc = 0;
+out:
+    free(d1); free(ss); free(gs); free(gstack); free(sstack); free(recs);
+    return rc;
+}
+
+int pb_topo_host_build(uint32_t cb, pb_topo_host_t *t) { return pb_topo_host_build_ex(cb, 0, t); }
+
+int pb_topo_host_build_ex(uint32_t cb, uint32_t csm, pb_topo_host_t *t)
 {
     memset(t, 0, sizeof(*t));
     uint64_t S64 = pb_copy_node_count(cb);
@@ -237,7 +314,6 @@ int pb_topo_host_build(uint32_t cb, pb_topo_host_t *t)
     for (uint32_t l = 0; l < L; l++) cntd[l + 1] += cntd[l];
     memcpy(cntl, cntd, (size_t)L * 4);
     for (uint32_t id = 0; id < S; id++) dorder[cntl[dies[id]]++] = id;
-    free(dies); dies = NULL;
 
     /* level-granular slot assignment: a level's nodes take slots before the
      * level's dying nodes release theirs */
@@ -252,11 +328,20 @@ int pb_topo_host_build(uint32_t cb, pb_topo_host_t *t)
             stack[top++] = slot[dorder[k]];
     }
     free(stack); stack = NULL;
+
+    /* id -> local output rank (kept in `stack`'s place) */
+    stack = (uint32_t *)malloc((size_t)S * 4);
+    if (!stack) goto out;
+    for (uint32_t id = 0; id < S; id++) stack[id] = PB_NO_RANK;
+    for (uint32_t r = 0; r < half_w; r++) stack[base[half_w + r]] = r;
+    if (csm && build_pipelined(S, L, np, p0, p1, lvl, dies, order, t->lstart, cntd, dorder, stack,
+                               csm, t) != 0)
+        goto out;
+    free(dies); dies = NULL;
     free(dorder); dorder = NULL;
 
     /* records; lvl is reused as the id -> local output rank map */
-    for (uint32_t id = 0; id < S; id++) lvl[id] = PB_NO_RANK;
-    for (uint32_t r = 0; r < half_w; r++) lvl[base[half_w + r]] = r;
+    memcpy(lvl, stack, (size_t)S * 4);
     t->recs = (uint32_t *)malloc((size_t)S * 16);
     t->orank = (uint32_t *)malloc((size_t)S * 4);
     if (!t->recs || !t->orank) goto out;

@@ -28,6 +28,29 @@ extern "C" {
 #define PB_NO_RANK 0xFFFFFFFFu
 #define PB_MAX_CHUNK_BLOCKS (1u << 20)
 
+/* Pipelined records (8 words per node, level order), built for a shared-
+ * memory label pool of `csm` slots per copy:
+ *   [0] x as above
+ *   [1] predecessor 0 reference, [2] predecessor 1 reference:
+ *       PB_REF_PREV = the predecessor was born at the previous level (it is
+ *       complete only after that level's barrier); PB_REF_SMEM = it lives in
+ *       the shared-memory pool; low 30 bits = its slot in that pool.  A
+ *       reference without PREV points at the global pool and may be fetched
+ *       one level early.
+ *   [3] global slot this node is copied to, PB_NO_SLOT if none (read by no
+ *       node two or more levels later, and by its next level through shared
+ *       memory)
+ *   [4] shared-memory slot this node is copied to, PB_NO_SLOT if none
+ *   [5] local output rank, PB_NO_RANK if not an output
+ *   [6], [7] zero
+ * A node's shared-memory copy lives for its own level and the next; nodes
+ * whose level has more next-level-read labels than the pool holds fall back
+ * to the global pool. */
+#define PB_REF_PREV (1u << 31)
+#define PB_REF_SMEM (1u << 30)
+#define PB_REF_SLOT_MASK 0x3FFFFFFFu
+#define PB_NO_SLOT 0xFFFFFFFFu
+
 typedef struct pb_topo_host {
     uint32_t cb;        /* chunk_blocks (m) */
     int n;              /* graph parameter n */
@@ -41,11 +64,18 @@ typedef struct pb_topo_host {
     uint32_t *recs;     /* [4 * S] packed records (x, y, z, w) */
     uint32_t *orank;    /* [S] local output rank per record, PB_NO_RANK otherwise */
     uint8_t desc[32];   /* graph descriptor digest */
+    /* pipelined layout (present when built with csm > 0) */
+    uint32_t csm;       /* shared-memory slots per copy */
+    uint32_t gpool2;    /* global slots per copy */
+    uint32_t *recs2;    /* [8 * S] pipelined records */
 } pb_topo_host_t;
 
 /* Build the schedule for chunk_blocks in [1, 2^20].  Returns 0, or -1 on a bad
  * argument or allocation failure (t is then left zeroed). */
 int pb_topo_host_build(uint32_t chunk_blocks, pb_topo_host_t *t);
+/* As pb_topo_host_build, plus the pipelined records for a shared-memory pool
+ * of csm slots per copy (csm = 0: none). */
+int pb_topo_host_build_ex(uint32_t chunk_blocks, uint32_t csm, pb_topo_host_t *t);
 void pb_topo_host_free(pb_topo_host_t *t);
 
 /* Nodes per copy and in a whole chunk (the reference's scaffold count). */

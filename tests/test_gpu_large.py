@@ -24,11 +24,14 @@ def test_plain_2e17_every_super_chunk(pkg, cuda, wl):
     cb, n = c["chunk_blocks"], c["chunks"]
     buf = cuda.zeros(n * cb * 32, dtype=cuda.uint8, device="cuda")
     with pkg.Topology(cb) as topo:
-        rc, st = topo.label(c["key"], buf.data_ptr(), n * cb * 32, c["rbo"], stats=True)
-        assert rc == 0, pkg.last_error()
-        assert digests(cuda, buf, cb * 32, n) == g["super_chunk_sha256"]
+        for kernel in (2, 1):
+            rc, st = topo.label(c["key"], buf.data_ptr(), n * cb * 32, c["rbo"],
+                                sched=pkg.Sched(kernel=kernel), stats=True)
+            assert rc == 0, pkg.last_error()
+            assert st["kernel"] == kernel
+            assert digests(cuda, buf, cb * 32, n) == g["super_chunk_sha256"], kernel
+            buf.zero_()
         # the block-0 table and in-register block 0 give the same bytes
-        buf.zero_()
     with pkg.Topology(cb, cv0_table=False) as topo:
         assert topo.label(c["key"], buf.data_ptr(), n * cb * 32, c["rbo"]) == 0
         assert digests(cuda, buf, cb * 32, n) == g["super_chunk_sha256"]

@@ -73,10 +73,32 @@ def test_plain_small_config(pkg, cuda, wl):
 def test_every_schedule_gives_the_same_bytes(pkg, cuda, wl, T, G):
     g = golden("configs.json")["plain_small"]
     c = wl.plain_small()
-    s = pkg.Sched(team_warps=T, units_per_team=G)
+    s = pkg.Sched(team_warps=T, units_per_team=G, kernel=1)
     got = label_region(pkg, cuda, c["key"], c["chunk_blocks"], c["chunks"], c["rbo"], sched=s,
                        cv0=(G % 2 == 0))
     assert hashlib.sha256(got).hexdigest() == g["region_sha256"]
+
+
+@pytest.mark.parametrize("T,G", [(4, 1), (8, 1), (16, 1), (4, 2), (8, 2), (16, 2)])
+def test_pipelined_kernel_gives_the_same_bytes(pkg, cuda, wl, oracle, T, G):
+    g = golden("configs.json")["plain_small"]
+    c = wl.plain_small()
+    s = pkg.Sched(team_warps=T, units_per_team=G, kernel=2)
+    got = label_region(pkg, cuda, c["key"], c["chunk_blocks"], c["chunks"], c["rbo"], sched=s)
+    assert hashlib.sha256(got).hexdigest() == g["region_sha256"]
+    for r in golden("small_regions.json"):
+        got = label_region(pkg, cuda, bytes.fromhex(r["key"]), r["chunk_blocks"], r["super_chunks"],
+                           r["rbo"], sched=s)
+        assert got.hex() == r["hex"], (r["chunk_blocks"], r["rbo"])
+
+
+def test_pipelined_kernel_with_few_teams(pkg, cuda, oracle):
+    rnd = random.Random(5)
+    for cb in (4096, 3000, 37):
+        key = rnd.randbytes(32)
+        s = pkg.Sched(team_warps=4, units_per_team=1, kernel=2, max_teams=3)
+        got = label_region(pkg, cuda, key, cb, 5, cb * 11, sched=s)
+        assert got == oracle.label_region(key, cb, 5, cb * 11, threads=8).tobytes(), cb
 
 
 def test_few_resident_teams_loop_over_the_queue(pkg, cuda, wl):
@@ -134,6 +156,7 @@ def test_stats_report_the_work(pkg, cuda):
     buf = dev_buffer(cuda, 8 * 1024 * 32)
     with pkg.Topology(1024) as topo:
         rc, st = topo.label(b"s" * 32, buf.data_ptr(), 8 * 1024 * 32, 0, stats=True)
+        assert st["kernel"] in (1, 2)
     assert rc == 0
     assert st["super_chunks"] == 8 and st["units"] == 16
     assert st["nodes"] == 8 * 96254

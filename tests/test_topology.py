@@ -26,7 +26,8 @@ class HostTopo(C.Structure):
     _fields_ = [("cb", C.c_uint32), ("n", C.c_int), ("half_w", C.c_uint32),
                 ("retained", C.c_uint32), ("S", C.c_uint32), ("L", C.c_uint32),
                 ("pool", C.c_uint32), ("max_width", C.c_uint32), ("lstart", u32p),
-                ("recs", u32p), ("orank", u32p), ("desc", C.c_uint8 * 32)]
+                ("recs", u32p), ("orank", u32p), ("desc", C.c_uint8 * 32),
+                ("csm", C.c_uint32), ("gpool2", C.c_uint32), ("recs2", u32p)]
 
 
 @pytest.fixture(scope="module")
@@ -43,6 +44,8 @@ def host():
     L.pb_topo_copy_edges.restype = C.c_uint64
     L.pb_topo_host_build.argtypes = [C.c_uint32, C.POINTER(HostTopo)]
     L.pb_topo_host_build.restype = C.c_int
+    L.pb_topo_host_build_ex.argtypes = [C.c_uint32, C.c_uint32, C.POINTER(HostTopo)]
+    L.pb_topo_host_build_ex.restype = C.c_int
     L.pb_topo_host_free.argtypes = [C.POINTER(HostTopo)]
     L.pb_chunk_seed.argtypes = [u8p, u8p, C.c_size_t, C.c_uint64]
     L.pb_graph_descriptor.argtypes = [u8p, C.c_uint64, C.c_uint64]
@@ -185,3 +188,88 @@ def test_bad_chunk_blocks(host):
     t = HostTopo()
     assert host.pb_topo_host_build(0, C.byref(t)) == -1
     assert host.pb_topo_host_build((1 << 20) + 1, C.byref(t)) == -1
+
+
+NO_SLOT = 0xFFFFFFFF
+PREV = 1 << 31
+SMEM = 1 << 30
+
+
+def pipelined(L, cb, csm):
+    t = HostTopo()
+    assert L.pb_topo_host_build_ex(cb, csm, C.byref(t)) == 0
+    lstart = np.ctypeslib.as_array(t.lstart, shape=(t.L + 1,)).copy()
+    recs2 = np.ctypeslib.as_array(t.recs2, shape=(t.S, 8)).copy()
+    recs = np.ctypeslib.as_array(t.recs, shape=(t.S, 4)).copy()
+    info = {k: getattr(t, k) for k in ("S", "L", "half_w", "csm", "gpool2", "pool")}
+    L.pb_topo_host_free(C.byref(t))
+    return info, lstart, recs, recs2
+
+
+@pytest.mark.parametrize("cb,csm", [(1, 4), (3, 2), (16, 4), (100, 16), (1024, 64), (1024, 4096),
+                                    (4096, 32), (4096, 2048)])
+def test_pipelined_records_are_safe(host, cb, csm):
+    """Simulate the pipelined schedule level by level with both pools:
+    every read sees its predecessor, no slot is written while it is read in the
+    same level, and a predecessor fetched one level early (a reference without
+    PREV) is not overwritten during the level in which it is fetched."""
+    info, lstart, recs, r2 = pipelined(host, cb, csm)
+    np_, p0, p1, outs = copy_edges(host, cb)
+    S, Lv = info["S"], info["L"]
+    assert info["csm"] <= csm
+    ids = (r2[:, 0] & 0x0FFFFFFF).astype(np.int64)
+    assert (r2[:, 0] == recs[:, 0]).all()
+    level = np.zeros(S, np.int64)
+    for l in range(Lv):
+        level[ids[lstart[l]:lstart[l + 1]]] = l
+    gs = r2[:, 3]
+    ss = r2[:, 4]
+    assert (gs[gs != NO_SLOT] < info["gpool2"]).all()
+    assert (ss[ss != NO_SLOT] < info["csm"]).all()
+    cg = np.full(max(1, info["gpool2"]), -1, np.int64)
+    cs = np.full(max(1, info["csm"]), -1, np.int64)
+
+    def check_ref(ref, pred, lv, early):
+        if (ref & PREV) != 0:
+            assert not early and level[pred] == lv - 1
+            pool = cs if (ref & SMEM) else cg
+        else:
+            assert level[pred] <= lv - 2
+            pool = cg
+        assert pool[ref & 0x3FFFFFFF] == pred
+
+    for l in range(Lv):
+        a, b = lstart[l], lstart[l + 1]
+        for k in range(a, b):
+            i = ids[k]
+            for e, pp in ((1, p0), (2, p1)):
+                if np_[i] >= e:
+                    check_ref(int(r2[k, e]), int(pp[i]), l, False)
+        # early fetch of the next level's old predecessors happens during level l
+        if l + 1 < Lv:
+            for k in range(lstart[l + 1], lstart[l + 2]):
+                i = ids[k]
+                for e, pp in ((1, p0), (2, p1)):
+                    if np_[i] >= e and (int(r2[k, e]) & PREV) == 0:
+                        check_ref(int(r2[k, e]), int(pp[i]), l + 1, True)
+                        assert int(r2[k, e]) not in set(gs[a:b].tolist())
+        gw = gs[a:b][gs[a:b] != NO_SLOT]
+        sw = ss[a:b][ss[a:b] != NO_SLOT]
+        assert len(set(gw.tolist())) == len(gw) and len(set(sw.tolist())) == len(sw)
+        reads_g, reads_s = set(), set()
+        for k in range(a, b):
+            for e in (1, 2):
+                if np_[ids[k]] >= e:
+                    ref = int(r2[k, e])
+                    (reads_s if (ref & PREV) and (ref & SMEM) else reads_g).add(ref & 0x3FFFFFFF)
+        assert not (reads_g & set(gw.tolist())) and not (reads_s & set(sw.tolist()))
+        for k in range(a, b):
+            i = ids[k]
+            if gs[k] != NO_SLOT:
+                cg[gs[k]] = i
+            if ss[k] != NO_SLOT:
+                cs[ss[k]] = i
+        # outputs keep their rank
+        outbit = (r2[a:b, 0] >> 30) & 1
+        assert ((r2[a:b, 5] != 0xFFFFFFFF) == (outbit == 1)).all()
+    assert info["gpool2"] <= info["pool"]
