@@ -68,6 +68,35 @@ int pose_b200_plan(const pose_hbm_topo_t *topo, uint64_t super_chunks,
  * latency of one compression in SM clocks (NULL to skip). */
 double pose_b200_compress_rate(uint32_t iters, double *latency_cycles);
 
+/* Labeling that allocates no device memory during the call.
+ *
+ * No counterpart in the reference: it is an addition of this library.  Same
+ * arguments, bytes and return convention as pose_graph_hbm_topo_label, for
+ * callers that must not call cudaMalloc while they label — e.g. a wipe worker
+ * that reserved the device's free memory for its label window before
+ * starting (a late allocation could fail half-way through a disk), or a host
+ * whose own allocator or an active stream capture forbids new device
+ * allocations.  The topology, seed and output buffer are still the caller's.
+ *
+ * Its scratch pool (64 MiB), chunk-seed table (8192 seeds) and work counter
+ * are static device arrays inside the library: a device holds them from when
+ * it loads them (at the latest, this function's first call on that device)
+ * until the process exits.  The schedule shrinks to fit 64 MiB, so every
+ * chunk_blocks in [1, 2^20] works; session seeds longer than 1016 bytes are
+ * rejected with an error, and buffers of more than 8192 super-chunks are
+ * labelled in several launches.
+ *
+ * The first call on a device looks up the arrays' device addresses
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the same arrays: the work counter is cleared by each launch
+ * and the scratch and seed table are zeroed before the call returns, but
+ * calls whose device work overlaps (from several host threads, or on several
+ * topologies of one device at once) race on them and must be serialised by
+ * the caller. */
+int pose_b200_topo_label_noalloc(const pose_hbm_topo_t *topo, const uint8_t *session_seed,
+                                 size_t seed_len, void *hbm_dev_ptr, size_t hbm_len,
+                                 uint64_t region_block_offset);
+
 /* Last error message of the calling thread ("" when none). */
 const char *pose_b200_last_error(void);
 

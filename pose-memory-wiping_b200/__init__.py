@@ -93,6 +93,9 @@ def _declare(L: C.CDLL) -> None:
     L.pose_b200_plan.restype = C.c_int
     L.pose_b200_compress_rate.argtypes = [C.c_uint32, C.POINTER(C.c_double)]
     L.pose_b200_compress_rate.restype = C.c_double
+    L.pose_b200_topo_label_noalloc.argtypes = [C.c_void_p, _u8p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                               C.c_uint64]
+    L.pose_b200_topo_label_noalloc.restype = C.c_int
     L.pose_b200_last_error.argtypes = []
     L.pose_b200_last_error.restype = C.c_char_p
 
@@ -159,6 +162,13 @@ class Topology:
                                     nbytes, region_block_offset,
                                     C.byref(sched) if sched is not None else None, C.byref(st))
         return (rc, st.as_dict()) if stats else rc
+
+    def label_noalloc(self, seed: bytes, dev_ptr: int, nbytes: int, region_block_offset: int = 0) -> int:
+        """pose_b200_topo_label_noalloc: the same bytes as label(), with the
+        library's static device scratch instead of memory allocated by the
+        call (for callers that cannot allocate while labeling)."""
+        return load().pose_b200_topo_label_noalloc(self.handle, _bytes_arg(seed), len(seed),
+                                                   C.c_void_p(dev_ptr), nbytes, region_block_offset)
 
     def plan(self, super_chunks: int, hint: Sched | None = None) -> Sched | None:
         out = Sched()

@@ -749,3 +749,33 @@ fail:
     if (b) cudaEventDestroy(b);
     return rate;
 }
+
+/* ── read-only access for the other translation units ────────────────────── */
+
+#include "topo_internal.h"
+
+int pb_topo_internal(const pose_hbm_topo_t *t, pb_topo_internal_t *out)
+{
+    if (!t || !out) return -1;
+    out->device = t->device;
+    out->cb = t->cb;
+    out->copies = t->copies;
+    out->super_bytes = t->super_bytes;
+    out->view = t->view;
+    out->stream = t->stream;
+    return 0;
+}
+
+int pb_plan_for_budget(const pose_hbm_topo_t *t, uint64_t nunits, uint64_t budget, pb_plan_out_t *out)
+{
+    /* the caller launches the basic lockstep kernel (k_label) with this plan */
+    pose_b200_sched_t basic;
+    memset(&basic, 0, sizeof(basic));
+    basic.kernel = 1;
+    plan_t p;
+    if (!t || !out || nunits == 0 || make_plan(t, nunits, &basic, budget, &p) != 0) return -1;
+    out->T = p.T; out->G = p.G; out->teams = p.teams; out->grid = p.grid; out->cta = p.cta;
+    out->team_scratch = p.team_scratch;
+    out->scratch_bytes = p.scratch_bytes;
+    return 0;
+}
