@@ -171,6 +171,108 @@ def run_reference_arm(args) -> None:
 
 # ── B200 arm ────────────────────────────────────────────────────────────────
 
+def run_batched(pkg, torch, sched=None, reps: int = 2) -> dict:
+    """The batched workload (256 sessions, chunk_blocks 2^12..2^17, 1-8 chunks
+    each at random absolute positions) through one persistent launch replayed
+    from a captured CUDA graph; MiB/s over the graph's device time."""
+    import pose_b200.workloads as wl
+    sessions = wl.batched()
+    topos = {cb: pkg.Topology(cb) for cb in sorted({s["chunk_blocks"] for s in sessions})}
+    total = sum(s["chunk_blocks"] * 32 * len(s["chunk_indices"]) for s in sessions)
+    big = torch.empty(total, dtype=torch.uint8, device="cuda")
+    reqs, off = [], 0
+    for s in sessions:
+        for idx in s["chunk_indices"]:
+            cb = s["chunk_blocks"]
+            reqs.append((topos[cb], s["key"], big.data_ptr() + off, cb * 32, idx * cb))
+            off += cb * 32
+    best = None
+    with pkg.Batch(reqs, sched) as b:
+        b.run()  # warm-up replay
+        for _ in range(reps):
+            rc, st = b.run()
+            assert rc == 0
+            if best is None or st["total_ms"] < best["total_ms"]:
+                best = st
+    for t in topos.values():
+        t.free()
+    return {"workload": "batched: 256 sessions x 1-8 chunks, chunk_blocks 2^12..2^17",
+            "value": total / MIB / (best["total_ms"] * 1e-3), "unit": "MiB/s",
+            "graph_ms": best["total_ms"], "super_chunks": best["super_chunks"], "units": best["units"],
+            "nodes": best["nodes"], "teams": best["teams"], "team_warps": best["team_warps"],
+            "max_units_per_team": best["units_per_team"], "kernel_launches_per_replay": 2}
+
+
+def run_served(pkg, torch, requests: int = 300, alone: bool = False) -> dict:
+    """Replay a fixed Poisson trace (200 requests/s from 64 sessions,
+    chunk_blocks 2^10..2^18, 1-16 chunks each) in real time against the
+    continuous-batching server; latency = submit to completion.  With alone,
+    the same requests also run one at a time (FIFO, each through
+    pose_graph_hbm_topo_label, latency = queueing on the same arrival times +
+    its measured service time)."""
+    import threading
+    import pose_b200.workloads as wl
+    trace = wl.served(requests)
+    topos = {cb: pkg.Topology(cb) for cb in sorted({r["chunk_blocks"] for r in trace})}
+    sizes = [r["chunks"] * r["chunk_blocks"] * 32 for r in trace]
+    big = torch.empty(sum(sizes), dtype=torch.uint8, device="cuda")
+    offs, o = [], 0
+    for sz in sizes:
+        offs.append(o)
+        o += sz
+    keys = {r["session"]: r["key"] for r in trace}
+    lat = [0.0] * len(trace)
+    with pkg.Server(scratch_bytes=32 << 30, max_waves=8) as srv:
+        sid = {s: srv.session(k) for s, k in keys.items()}
+        tickets = [None] * len(trace)
+        t0 = time.perf_counter()
+
+        def feeder():
+            for i, r in enumerate(trace):
+                d = r["arrival_s"] - (time.perf_counter() - t0)
+                if d > 0:
+                    time.sleep(d)
+                tickets[i] = srv.submit(topos[r["chunk_blocks"]], sid[r["session"]], big.data_ptr() + offs[i],
+                                        sizes[i], r["first_chunk"] * r["chunk_blocks"])
+
+        th = threading.Thread(target=feeder)
+        th.start()
+        th.join()
+        for i, tk in enumerate(tickets):
+            rc, q, tot = srv.wait(tk)
+            assert rc == 0
+            lat[i] = tot
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+    lat_sorted = sorted(lat)
+    out = {"workload": f"served: Poisson 200 req/s, 64 sessions, {len(trace)} requests, chunk_blocks 2^10..2^18",
+           "value": sum(sizes) / MIB / wall, "unit": "MiB/s", "p50_ms": lat_sorted[len(lat) // 2],
+           "p99_ms": lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))], "waves": st["waves"],
+           "offered_mib_s": sum(sizes) / MIB / trace[-1]["arrival_s"], "wall_s": wall}
+    if alone:
+        # one request at a time, FIFO, on the same arrival times
+        sub = trace
+        clock = 0.0
+        lat1 = []
+        for i, r in enumerate(sub):
+            start = max(clock, r["arrival_s"])
+            torch.cuda.synchronize()
+            a = time.perf_counter()
+            rc = topos[r["chunk_blocks"]].label(r["key"], big.data_ptr() + offs[i], sizes[i],
+                                                r["first_chunk"] * r["chunk_blocks"])
+            torch.cuda.synchronize()
+            svc = time.perf_counter() - a
+            assert rc == 0
+            clock = start + svc
+            lat1.append((clock - r["arrival_s"]) * 1e3)
+        l1 = sorted(lat1)
+        out["one_at_a_time"] = {"requests": len(sub), "value": sum(sizes) / MIB / clock, "unit": "MiB/s",
+                                "p50_ms": l1[len(l1) // 2], "p99_ms": l1[min(len(l1) - 1, int(0.99 * len(l1)))]}
+    for t in topos.values():
+        t.free()
+    return out
+
+
 def run_b200(args) -> None:
     import torch
     pkg = load_pkg()
@@ -189,7 +291,8 @@ def run_b200(args) -> None:
     cb, nsup = w["chunk_blocks"], w["chunks"]
     sb = cb * 32
     nbytes = nsup * sb
-    rbo = w["rbo"] + rank * nsup * cb  # each rank: its own disjoint absolute range
+    import pose_b200.workloads as wl
+    rbo, nsup = wl.rank_region(w, rank, world)  # each rank: its own disjoint absolute range
 
     def barrier():
         torch.cuda.synchronize()
@@ -275,6 +378,9 @@ def run_b200(args) -> None:
         "clocks": clocks,
         "kernel_ms": kernel_ms,
     }
+    if world == 1 and not args.no_aux and args.workload == "plain_2e17":
+        line["batched"] = run_batched(pkg, torch)
+        line["served"] = run_served(pkg, torch, requests=120, alone=True)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             cpu = cpu_reference(w, 1, 0)
@@ -290,6 +396,20 @@ def run_b200(args) -> None:
         dist.destroy_process_group()
 
 
+def run_aux(args) -> None:
+    """--workload batched | served: one JSON line for that form alone."""
+    import torch
+    pkg = load_pkg()
+    os.environ.setdefault("POSE_GPU_QUIET", "1")
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if args.workload == "batched":
+        r = run_batched(pkg, torch, reps=max(1, args.steps))
+    else:
+        r = run_served(pkg, torch, requests=args.requests, alone=args.alone)
+    r.update({"metric": "label MiB/s", "n_gpus": 1, "impl": "b200", "data": "synthetic (splitmix64 session keys)"})
+    print(json.dumps(r), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -299,9 +419,14 @@ def main() -> None:
     ap.add_argument("--workload", default="plain_2e17")
     ap.add_argument("--no-cv0", action="store_true", help="hash block 0 in every call (no table)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-aux", action="store_true", help="skip the batched and served legs")
+    ap.add_argument("--requests", type=int, default=300, help="served: trace length")
+    ap.add_argument("--alone", action="store_true", help="served: also run the trace one request at a time")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.workload in ("batched", "served"):
+        run_aux(args)
     else:
         run_b200(args)
 

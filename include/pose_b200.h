@@ -23,8 +23,12 @@ typedef struct {
     uint32_t team_warps;        /* T: warps that cooperate on one batch (1..16, power of 2) */
     uint32_t units_per_team;    /* G: chunk copies run in lockstep by one team (1..32, power of 2) */
     uint32_t max_teams;         /* cap on resident teams (0 = occupancy and memory bound) */
-    uint32_t kernel;            /* 0 = automatic, 1 = basic lockstep kernel, 2 = pipelined kernel */
+    uint32_t kernel;            /* 0 = automatic, 1 = basic lockstep kernel, 2 = pipelined kernel,
+                                   3 = warp-specialised kernel (team_warps = hashing warps: 7 or 15) */
     uint64_t scratch_cap_bytes; /* cap on the scratch pool (0 = free HBM less a margin) */
+    uint32_t lane_efficiency;   /* batched launches: per-topology G reaches this lane efficiency,
+                                   in percent (0 = automatic) */
+    uint32_t reserved;
 } pose_b200_sched_t;
 
 /* What one call did (device times from CUDA events on the labeler's stream). */
@@ -37,7 +41,8 @@ typedef struct {
     uint64_t scratch_bytes;     /* scratch pool bytes used */
     uint32_t team_warps, units_per_team, teams, kernel_launches;
     uint32_t used_cv0_table;    /* 1 when block 0 came from the precomputed table */
-    uint32_t kernel;            /* 1 = basic lockstep kernel, 2 = pipelined kernel */
+    uint32_t kernel;            /* 1 = basic lockstep kernel, 2 = pipelined kernel, 3 = warp-specialised,
+                                   4 = multi-topology batch kernel */
 } pose_b200_stats_t;
 
 /* Extends pose_graph_hbm_topo_build (common/include/gpu_label.h:77-78).
@@ -67,6 +72,149 @@ int pose_b200_plan(const pose_hbm_topo_t *topo, uint64_t super_chunks,
  * compressions per second (0 on error); *latency_cycles gets the dependent
  * latency of one compression in SM clocks (NULL to skip). */
 double pose_b200_compress_rate(uint32_t iters, double *latency_cycles);
+
+/* ── batched labeling ────────────────────────────────────────────────────
+ *
+ * Extends pose_graph_hbm_topo_label (common/include/gpu_label.h:80-83) to many
+ * requests at once: each request is one session seed, one topology (one
+ * chunk_blocks), one device buffer and one region_block_offset, with exactly
+ * the semantics of a pose_graph_hbm_topo_label call on it; all requests run
+ * in ONE persistent kernel launch (teams take same-topology batches from a
+ * device queue, longest first), replayed from a captured CUDA graph.  All
+ * topologies must belong to the current device.  Bytes are identical to
+ * labelling each request alone. */
+typedef struct {
+    const pose_hbm_topo_t *topo;
+    const uint8_t *session_seed;
+    size_t seed_len;
+    void *hbm_dev_ptr;
+    size_t hbm_len;
+    uint64_t region_block_offset;
+} pose_b200_request_t;
+
+typedef struct pose_b200_batch pose_b200_batch_t;
+
+/* Plan, upload and capture; NULL on error.  The requests' seeds are copied;
+ * their buffers must stay valid until the batch is destroyed.  sched may fix
+ * team_warps (1, 2, 4 or 8) and lane_efficiency, and cap units_per_team (the
+ * largest G), max_teams and scratch_cap_bytes; what it leaves at 0 is chosen
+ * by the makespan estimate. */
+pose_b200_batch_t *pose_b200_batch_create(const pose_b200_request_t *reqs, size_t n,
+                                          const pose_b200_sched_t *sched);
+/* Replay the captured launch (synchronous).  0 on success, -1 on error. */
+int pose_b200_batch_run(pose_b200_batch_t *batch, pose_b200_stats_t *stats);
+/* Zero the batch's scratch and seeds, free it. */
+void pose_b200_batch_destroy(pose_b200_batch_t *batch);
+/* create + run + destroy. */
+int pose_b200_label_batch(const pose_b200_request_t *reqs, size_t n, const pose_b200_sched_t *sched,
+                          pose_b200_stats_t *stats);
+
+/* ── streaming to a host sink ────────────────────────────────────────────
+ *
+ * Sink of labelled bytes, the shape of the reference's pose_label_sink_fn
+ * (common/include/graph.h:244-245): called once per window with the pinned
+ * host buffer holding it, its length and its absolute byte offset in the
+ * target; returns 0 on success, non-zero to abort.  It is called from a
+ * worker thread, one window at a time, in order. */
+typedef int (*pose_b200_sink_fn)(void *ctx, const uint8_t *buf, size_t len, uint64_t off);
+
+/* Label floor(region_bytes / (chunk_blocks*32)) super-chunks starting at
+ * block offset region_block_offset (chunk index as in
+ * pose_graph_hbm_topo_label) and deliver them to `sink` window by window
+ * (window_bytes rounded down to whole super-chunks, at least one): window
+ * k+1 is labelled on the GPU while window k is copied to pinned host memory
+ * and sunk, which the reference's disk worker does one after the other
+ * (tools/disk-wipe-bench/disk_wipe_bench.cu:646-697).  `off` of window k is
+ * byte_offset + k*window.  Synchronous; 0 on success, -1 on error (including
+ * a failing sink). */
+int pose_b200_label_stream(const pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
+                           uint64_t region_bytes, uint64_t region_block_offset, uint64_t byte_offset,
+                           size_t window_bytes, pose_b200_sink_fn sink, void *sink_ctx,
+                           const pose_b200_sched_t *sched, pose_b200_stats_t *stats);
+
+/* ── continuous-batching server ──────────────────────────────────────────
+ *
+ * A labeling service for many concurrent requests.  Session seeds are kept in
+ * device memory; requests (the arguments of pose_graph_hbm_topo_label, with a
+ * session instead of a seed) can be submitted from any thread at any time.  A
+ * dispatcher thread admits the oldest pending requests into a wave — one
+ * persistent multi-topology launch on its own stream — whenever a wave slot
+ * is free and the scratch arena (the HBM budget given at creation) has room,
+ * so work that arrives while other waves run starts as memory frees up and
+ * overlaps them on the device.  Each result is byte-identical to labelling
+ * the request alone.  All topologies and buffers must be on the device that
+ * was current at creation. */
+typedef struct pose_b200_server pose_b200_server_t;
+
+/* scratch_bytes: HBM arena for all waves (0 = half the free memory);
+ * max_waves: concurrent waves (0 = 4, at most 16).  NULL on error. */
+pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max_waves);
+/* Register a session seed (<= 1016 bytes); returns its id, or -1. */
+int pose_b200_server_session(pose_b200_server_t *server, const uint8_t *seed, size_t seed_len);
+/* Queue one request; returns its ticket, or -1. */
+int64_t pose_b200_server_submit(pose_b200_server_t *server, const pose_hbm_topo_t *topo, int session,
+                                void *hbm_dev_ptr, size_t hbm_len, uint64_t region_block_offset);
+/* Block until the request finished: 0 on success, -1 on failure; queue_ms
+ * (submit to launch) and total_ms (submit to completion) may be NULL. */
+int pose_b200_server_wait(pose_b200_server_t *server, int64_t ticket, double *queue_ms, double *total_ms);
+/* 1 done, 0 pending or running, -1 failed or unknown. */
+int pose_b200_server_query(pose_b200_server_t *server, int64_t ticket);
+void pose_b200_server_stats(pose_b200_server_t *server, uint64_t *submitted, uint64_t *waves,
+                            uint64_t *scratch_bytes);
+/* Finish all submitted work, zero the arena and the session seeds, free. */
+void pose_b200_server_destroy(pose_b200_server_t *server);
+
+/* ── verifier: challenge recompute on the GPU ────────────────────────────── */
+
+/* pose_graph_challenge (common/include/graph.h:99-102, common/src/graph.c:
+ * 1019-1042) on the GPU: the label of output rank challenge_idx of the graph
+ * of m = the topology's chunk_blocks outputs, labelled with `seed` as its
+ * graph seed.  As in the reference, that seed is a chunk seed (for a region,
+ * pose_chunk_seed(session seed, chunk index)) and only its first 32 bytes are
+ * used.  The reference labels the whole graph on the CPU; here the chunk is
+ * labelled on the device (both standalone copies run side by side, so the
+ * latency is that of one copy) and 32 bytes come back.  0 on success; -1 when
+ * challenge_idx >= m, seed is NULL or shorter than 32 bytes, or on a CUDA
+ * error. */
+int pose_b200_challenge(const pose_hbm_topo_t *topo, const uint8_t *seed, size_t seed_len,
+                        uint64_t challenge_idx, uint8_t out[32]);
+
+/* Many challenges of one session at once.  blocks[k] is an absolute block
+ * index of a labelled region (the unit of region_block_offset): output rank
+ * blocks[k] % cb of chunk blocks[k] / cb, whose chunk seed is
+ * pose_chunk_seed(session_seed, blocks[k] / cb) (common/src/graph.c:
+ * 1646-1649).  Each distinct chunk is recomputed once; the chunks run as
+ * batched launches of at most 4 GiB of labels each, and out[32k..32k+31]
+ * receives the label of blocks[k].  sched as for pose_b200_batch_create;
+ * session seeds of at most 1016 bytes.
+ * 0 on success, -1 on error. */
+int pose_b200_challenge_blocks(const pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
+                               const uint64_t *blocks, size_t n, uint8_t *out,
+                               const pose_b200_sched_t *sched, pose_b200_stats_t *stats);
+
+/* Reads len bytes at byte offset off of the labelled target into buf, like
+ * the pread of the reference's verify step; returns 0 on success. */
+typedef int (*pose_b200_read_fn)(void *ctx, uint8_t *buf, size_t len, uint64_t off);
+
+/* The sampled verify of disk-wipe-bench (verify_disk,
+ * tools/disk-wipe-bench/disk_wipe_bench.cu:300-366) with the recompute on the
+ * GPU.  The target holds n_super = wipe_len / (cb*32) super-chunks labelled
+ * from region block 0 (super-chunk J at byte J*cb*32, chunk index J).
+ * `samples` of them (clamped to [1, n_super]; J_k = k*(n_super-1)/(samples-1),
+ * first and last included) are read through `read`, recomputed on the GPU in
+ * batched launches while the reads run, and compared on the device (session
+ * seeds of at most 1016 bytes).
+ * *checked and *mismatched count super-chunks (either may be NULL);
+ * first_bad, when not NULL, has `samples` entries and receives each sample's
+ * first mismatching block within its super-chunk, or UINT64_MAX when it
+ * matched.  The first three mismatches are also printed to stderr, as the
+ * reference does.  0 when setup and I/O succeeded (mismatches are results,
+ * not errors); -1 when nothing was labelled, a read failed, or on a CUDA
+ * error. */
+int pose_b200_verify_sampled(const pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
+                             uint64_t wipe_len, uint64_t samples, pose_b200_read_fn read, void *read_ctx,
+                             uint64_t *checked, uint64_t *mismatched, uint64_t *first_bad,
+                             const pose_b200_sched_t *sched, pose_b200_stats_t *stats);
 
 /* Labeling that allocates no device memory during the call.
  *

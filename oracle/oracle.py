@@ -179,6 +179,8 @@ class RefCPU:
         L.pose_graph_scaffold_node_count.restype = C.c_uint64
         L.pose_graph_label.argtypes = [_u8p, C.c_size_t, C.c_uint64, _u8p, C.c_int]
         L.pose_graph_label.restype = C.c_int
+        L.pose_graph_challenge.argtypes = [_u8p, C.c_size_t, C.c_uint64, C.c_uint64, _u8p, C.c_int]
+        L.pose_graph_challenge.restype = C.c_int
         L.pose_graph_slot_map.argtypes = [C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
         L.pose_graph_slot_map.restype = C.c_int
         self.L = L
@@ -245,3 +247,10 @@ class RefCPU:
         s = _buf(seed)
         assert self.L.pose_graph_label(s[0], len(seed), m, out.ctypes.data_as(_u8p), 0) == 0
         return out
+
+    def challenge(self, seed: bytes, m: int, idx: int) -> bytes | None:
+        """The reference's pose_graph_challenge (verifier recompute)."""
+        out = np.zeros(32, np.uint8)
+        s = _buf(seed)
+        rc = self.L.pose_graph_challenge(s[0], len(seed), m, idx, out.ctypes.data_as(_u8p), 0)
+        return out.tobytes() if rc == 0 else None

@@ -37,7 +37,8 @@ class Sched(C.Structure):
 
     _fields_ = [("team_warps", C.c_uint32), ("units_per_team", C.c_uint32),
                 ("max_teams", C.c_uint32), ("kernel", C.c_uint32),
-                ("scratch_cap_bytes", C.c_uint64)]
+                ("scratch_cap_bytes", C.c_uint64), ("lane_efficiency", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class Stats(C.Structure):
@@ -54,8 +55,17 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Request(C.Structure):
+    """pose_b200_request_t: one pose_graph_hbm_topo_label-style request."""
+
+    _fields_ = [("topo", C.c_void_p), ("session_seed", C.c_void_p), ("seed_len", C.c_size_t),
+                ("hbm_dev_ptr", C.c_void_p), ("hbm_len", C.c_size_t), ("region_block_offset", C.c_uint64)]
+
+
 _u8p = C.POINTER(C.c_uint8)
 _u32p = C.POINTER(C.c_uint32)
+SINK_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint64)
+READ_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint64)
 
 
 def build(force: bool = False) -> str:
@@ -96,6 +106,41 @@ def _declare(L: C.CDLL) -> None:
     L.pose_b200_topo_label_noalloc.argtypes = [C.c_void_p, _u8p, C.c_size_t, C.c_void_p, C.c_size_t,
                                                C.c_uint64]
     L.pose_b200_topo_label_noalloc.restype = C.c_int
+    L.pose_b200_batch_create.argtypes = [C.POINTER(Request), C.c_size_t, C.POINTER(Sched)]
+    L.pose_b200_batch_create.restype = C.c_void_p
+    L.pose_b200_batch_run.argtypes = [C.c_void_p, C.POINTER(Stats)]
+    L.pose_b200_batch_run.restype = C.c_int
+    L.pose_b200_batch_destroy.argtypes = [C.c_void_p]
+    L.pose_b200_batch_destroy.restype = None
+    L.pose_b200_label_batch.argtypes = [C.POINTER(Request), C.c_size_t, C.POINTER(Sched), C.POINTER(Stats)]
+    L.pose_b200_label_batch.restype = C.c_int
+    L.pose_b200_label_stream.argtypes = [C.c_void_p, _u8p, C.c_size_t, C.c_uint64, C.c_uint64, C.c_uint64,
+                                         C.c_size_t, SINK_FN, C.c_void_p, C.POINTER(Sched), C.POINTER(Stats)]
+    L.pose_b200_label_stream.restype = C.c_int
+    L.pose_b200_server_create.argtypes = [C.c_uint64, C.c_uint32]
+    L.pose_b200_server_create.restype = C.c_void_p
+    L.pose_b200_server_session.argtypes = [C.c_void_p, _u8p, C.c_size_t]
+    L.pose_b200_server_session.restype = C.c_int
+    L.pose_b200_server_submit.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_uint64]
+    L.pose_b200_server_submit.restype = C.c_int64
+    L.pose_b200_server_wait.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.pose_b200_server_wait.restype = C.c_int
+    L.pose_b200_server_query.argtypes = [C.c_void_p, C.c_int64]
+    L.pose_b200_server_query.restype = C.c_int
+    L.pose_b200_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                         C.POINTER(C.c_uint64)]
+    L.pose_b200_server_stats.restype = None
+    L.pose_b200_server_destroy.argtypes = [C.c_void_p]
+    L.pose_b200_server_destroy.restype = None
+    L.pose_b200_challenge.argtypes = [C.c_void_p, _u8p, C.c_size_t, C.c_uint64, _u8p]
+    L.pose_b200_challenge.restype = C.c_int
+    L.pose_b200_challenge_blocks.argtypes = [C.c_void_p, _u8p, C.c_size_t, C.POINTER(C.c_uint64), C.c_size_t,
+                                             _u8p, C.POINTER(Sched), C.POINTER(Stats)]
+    L.pose_b200_challenge_blocks.restype = C.c_int
+    L.pose_b200_verify_sampled.argtypes = [C.c_void_p, _u8p, C.c_size_t, C.c_uint64, C.c_uint64, READ_FN,
+                                           C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                           C.POINTER(C.c_uint64), C.POINTER(Sched), C.POINTER(Stats)]
+    L.pose_b200_verify_sampled.restype = C.c_int
     L.pose_b200_last_error.argtypes = []
     L.pose_b200_last_error.restype = C.c_char_p
 
@@ -170,6 +215,70 @@ class Topology:
         return load().pose_b200_topo_label_noalloc(self.handle, _bytes_arg(seed), len(seed),
                                                    C.c_void_p(dev_ptr), nbytes, region_block_offset)
 
+    def label_stream(self, seed: bytes, region_bytes: int, sink, region_block_offset: int = 0,
+                     byte_offset: int = 0, window_bytes: int = 1 << 30, sched: Sched | None = None):
+        """pose_b200_label_stream: label region_bytes worth of super-chunks and
+        call sink(memoryview, off) per window (from a worker thread) while the
+        next window is labelled.  Returns (rc, stats dict)."""
+        def _cb(ctx, buf, n, off):
+            try:
+                return int(sink(memoryview((C.c_uint8 * n).from_address(buf)), off) or 0)
+            except Exception:
+                return -1
+        cb = SINK_FN(_cb)
+        st = Stats()
+        rc = load().pose_b200_label_stream(self.handle, _bytes_arg(seed), len(seed), region_bytes,
+                                           region_block_offset, byte_offset, window_bytes, cb, None,
+                                           C.byref(sched) if sched is not None else None, C.byref(st))
+        return rc, st.as_dict()
+
+    def challenge(self, seed: bytes, challenge_idx: int) -> bytes | None:
+        """pose_b200_challenge: the label of output rank challenge_idx of the
+        chunk graph labelled with `seed` (a 32-byte chunk seed), as the
+        reference's pose_graph_challenge; None when the call fails."""
+        out = (C.c_uint8 * 32)()
+        rc = load().pose_b200_challenge(self.handle, _bytes_arg(seed), len(seed), challenge_idx,
+                                        C.cast(out, _u8p))
+        return bytes(out) if rc == 0 else None
+
+    def challenge_blocks(self, session_seed: bytes, blocks, sched: Sched | None = None):
+        """pose_b200_challenge_blocks: labels of absolute region blocks of one
+        session.  Returns (rc, labels as n*32 bytes, stats dict)."""
+        blocks = list(blocks)
+        arr = (C.c_uint64 * max(1, len(blocks)))(*blocks)
+        out = (C.c_uint8 * max(1, 32 * len(blocks)))()
+        st = Stats()
+        rc = load().pose_b200_challenge_blocks(self.handle, _bytes_arg(session_seed), len(session_seed), arr,
+                                               len(blocks), C.cast(out, _u8p),
+                                               C.byref(sched) if sched is not None else None, C.byref(st))
+        return rc, bytes(out)[:32 * len(blocks)], st.as_dict()
+
+    def verify_sampled(self, session_seed: bytes, wipe_len: int, samples: int, read,
+                       sched: Sched | None = None) -> dict:
+        """pose_b200_verify_sampled with read(nbytes, off) -> bytes-like giving
+        the stored bytes at byte offset off.  Returns a dict with rc, checked,
+        mismatched, first_bad (per sample, None where it matched) and stats."""
+        def _cb(ctx, buf, n, off):
+            try:
+                data = read(n, off)
+                if data is None or len(data) != n:
+                    return -1
+                C.memmove(buf, bytes(data), n)
+                return 0
+            except Exception:
+                return -1
+        cb = READ_FN(_cb)
+        checked, mism = C.c_uint64(), C.c_uint64()
+        fb = (C.c_uint64 * max(1, samples))()
+        st = Stats()
+        rc = load().pose_b200_verify_sampled(self.handle, _bytes_arg(session_seed), len(session_seed), wipe_len,
+                                             samples, cb, None, C.byref(checked), C.byref(mism), fb,
+                                             C.byref(sched) if sched is not None else None, C.byref(st))
+        n = max(1, min(samples, wipe_len // self.super_bytes)) if wipe_len >= self.super_bytes else 0
+        return {"rc": rc, "checked": checked.value, "mismatched": mism.value,
+                "first_bad": [None if fb[i] == (1 << 64) - 1 else fb[i] for i in range(min(n, samples))],
+                "stats": st.as_dict()}
+
     def plan(self, super_chunks: int, hint: Sched | None = None) -> Sched | None:
         out = Sched()
         rc = load().pose_b200_plan(self.handle, super_chunks,
@@ -190,6 +299,98 @@ class Topology:
     def __del__(self):
         try:
             self.free()
+        except Exception:
+            pass
+
+
+class Batch:
+    """pose_b200_batch_t: many requests in one persistent launch, captured once
+    into a CUDA graph and replayed by run().
+
+    requests: iterable of (topology, seed bytes, device pointer, nbytes, rbo)."""
+
+    def __init__(self, requests, sched: Sched | None = None):
+        reqs = list(requests)
+        self._seeds = [C.create_string_buffer(bytes(r[1]), max(1, len(r[1]))) for r in reqs]
+        arr = (Request * len(reqs))()
+        for i, (topo, seed, ptr, nbytes, rbo) in enumerate(reqs):
+            arr[i] = Request(topo.handle, C.cast(self._seeds[i], C.c_void_p), len(seed), ptr, nbytes, rbo)
+        self._arr = arr
+        h = load().pose_b200_batch_create(arr, len(reqs), C.byref(sched) if sched is not None else None)
+        if not h:
+            raise RuntimeError("batch create failed")
+        self.handle = h
+
+    def run(self) -> tuple[int, dict]:
+        st = Stats()
+        rc = load().pose_b200_batch_run(self.handle, C.byref(st))
+        return rc, st.as_dict()
+
+    def free(self) -> None:
+        if self.handle:
+            load().pose_b200_batch_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.free()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Server:
+    """pose_b200_server_t: continuous-batching labeling service."""
+
+    def __init__(self, scratch_bytes: int = 0, max_waves: int = 0):
+        h = load().pose_b200_server_create(scratch_bytes, max_waves)
+        if not h:
+            raise RuntimeError("server create failed")
+        self.handle = h
+
+    def session(self, seed: bytes) -> int:
+        sid = load().pose_b200_server_session(self.handle, _bytes_arg(seed), len(seed))
+        if sid < 0:
+            raise RuntimeError("session registration failed")
+        return sid
+
+    def submit(self, topo: "Topology", session: int, dev_ptr: int, nbytes: int, rbo: int = 0) -> int:
+        return load().pose_b200_server_submit(self.handle, topo.handle, session, C.c_void_p(dev_ptr), nbytes, rbo)
+
+    def wait(self, ticket: int) -> tuple[int, float, float]:
+        """(rc, queue_ms, total_ms) of one request."""
+        q = C.c_double()
+        t = C.c_double()
+        rc = load().pose_b200_server_wait(self.handle, ticket, C.byref(q), C.byref(t))
+        return rc, q.value, t.value
+
+    def query(self, ticket: int) -> int:
+        return load().pose_b200_server_query(self.handle, ticket)
+
+    def stats(self) -> dict:
+        a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        load().pose_b200_server_stats(self.handle, C.byref(a), C.byref(b), C.byref(c))
+        return {"submitted": a.value, "waves": b.value, "scratch_bytes": c.value}
+
+    def close(self) -> None:
+        if self.handle:
+            load().pose_b200_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass
 

@@ -14,6 +14,12 @@ extern "C" {
 
 /* Largest CTA the labeling kernel is launched with (teams of up to 16 warps). */
 #define PB_CTA_THREADS 512
+/* Largest CTA of the multi-topology kernel (k_label_multi is compiled for
+ * three such CTAs per SM). */
+#define PB_MULTI_CTA_THREADS 256
+/* Dynamic shared memory of k_label / k_label_multi per thread: two staging
+ * buffers of one node's record and block-0 chaining value (48 bytes each). */
+#define PB_PREF_BYTES_PER_THREAD 96u
 
 #ifdef __CUDACC__
 typedef uint4 pb_u4;
@@ -53,6 +59,46 @@ typedef struct {
     uint32_t one;                /* must be 1 */
 } pb_label_params_t;
 
+/* Multi-topology launch (batched sessions): batch b runs units
+ * [first_unit, first_unit + count) of topology `topo`, count <= 2^glog. */
+typedef struct {
+    uint32_t topo, first_unit, count, glog;
+} pb_mbatch_t;
+
+typedef struct {
+    uint64_t out;   /* device address of the unit's persisted super-chunk */
+    uint32_t seed;  /* index of its chunk seed in the seed table */
+    uint32_t copy;  /* 0 = left copy, 1 = right copy */
+} pb_munit_t;
+
+typedef struct {
+    uint64_t chunk_index;
+    uint32_t seed_off, seed_len; /* session seed in the seed blob */
+} pb_seedjob_t;
+
+typedef struct {
+    const pb_topo_view_t *topos;
+    const pb_mbatch_t *batches;
+    const pb_munit_t *units;
+    const uint32_t *seeds;
+    uint8_t *scratch;
+    uint64_t team_scratch_bytes;
+    uint32_t nbatches;
+    uint32_t team_warps;
+    unsigned int *queue;
+    uint32_t fma_adds;
+    uint32_t one;
+    /* optional completion signal: when a batch finishes, each of its units
+     * adds 1 to req_done[unit_req[unit]] (system-scope, after a system
+     * fence), so the host sees every request end as it happens */
+    const uint32_t *unit_req;
+    unsigned int *req_done;
+} pb_multi_params_t;
+
+int pb_dev_label_multi(const pb_multi_params_t *params, uint32_t grid, uint32_t cta_threads, cudaStream_t stream);
+int pb_dev_label_multi_occupancy(uint32_t cta_threads, int *blocks_per_sm);
+int pb_dev_seed_jobs(const void *jobs, uint32_t njobs, const uint8_t *blob, uint32_t *seeds, cudaStream_t stream);
+
 /* Device view of the pipelined records (topology.h, PB_REF_*). */
 typedef struct {
     const pb_u4 *recs2;      /* [2 * S] pipelined records, level order */
@@ -88,6 +134,20 @@ typedef struct {
 int pb_dev_label_pipe(const pb_pipe_params_t *params, uint32_t grid, uint32_t cta_threads,
                       uint32_t smem_bytes, cudaStream_t stream);
 int pb_dev_label_pipe_occupancy(uint32_t cta_threads, uint32_t smem_bytes, int *blocks_per_sm);
+
+/* Warp-specialised depth-regime kernel (label_ws.cu): team_warps hashing
+ * warps + 1 producer warp per CTA, one chunk copy per CTA, g_log2 = 0. */
+int pb_dev_label_ws(const pb_pipe_params_t *params, uint32_t grid, uint32_t cta_threads,
+                    uint32_t smem_bytes, cudaStream_t stream);
+int pb_dev_label_ws_occupancy(uint32_t cta_threads, uint32_t smem_bytes, int *blocks_per_sm);
+
+/* Verifier helpers (label_verify.cu).  Compare nblocks 32-byte blocks of a
+ * and b, grouped blocks_per_group to a group: first_bad[g] = min over
+ * mismatching blocks of their index within group g (initialise it to all
+ * ones).  Gather: out[k] = the 32-byte label at block src[k] of work. */
+int pb_dev_compare_blocks(const void *a, const void *b, uint64_t nblocks, uint64_t blocks_per_group,
+                          unsigned long long *first_bad, uint32_t grid, cudaStream_t stream);
+int pb_dev_gather_labels(const void *work, const uint64_t *src, uint32_t n, void *out, cudaStream_t stream);
 
 int pb_dev_set_keys(const uint32_t ksrc[8], const uint32_t kint[8], const uint32_t kseed[8]);
 int pb_dev_cv0_table(const void *recs, uint32_t S, uint32_t copies, void *cv0, cudaStream_t stream);

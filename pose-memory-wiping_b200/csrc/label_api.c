@@ -79,6 +79,7 @@ struct pose_hbm_topo {
     pb_topo_view_t view;
     pb_topo_view2_t view2; /* pipelined records (d_recs2 != NULL) */
     int occ_pipe[5][2];    /* pipelined kernel CTAs/SM for T = 1..16, G = 1, 2 (-1 = not queried) */
+    int occ_ws[2];         /* warp-specialised kernel CTAs/SM for 7 and 15 hashing warps */
     /* per-topology workspace, reused across calls (one caller thread at a time) */
     cudaStream_t stream;
     cudaEvent_t ev[4];
@@ -132,6 +133,38 @@ static uint32_t pipe_smem_bytes(const pose_hbm_topo_t *t, uint32_t T, uint32_t G
     return t->view2.csm * G * 32u + 32u * T * PB_PIPE_STAGE_BYTES_PER_THREAD;
 }
 
+static double model_ws_latency(void)
+{
+    const char *e = getenv("POSE_B200_WS_LATENCY");
+    double v = e ? atof(e) : 0.0;
+    return v > 0 ? v : 2700.0;
+}
+
+static uint32_t ws_smem_bytes(const pose_hbm_topo_t *t, uint32_t nc)
+{
+    return (2u * t->view2.csm + 18u * 32u * nc + 3u) * 16u;
+}
+
+static int ws_occupancy(pose_hbm_topo_t *t, uint32_t nc)
+{
+    int i = nc == 7 ? 0 : 1;
+    if (t->occ_ws[i] < 0) {
+        int occ = 0;
+        uint32_t smem = ws_smem_bytes(t, nc);
+        if (smem > 227u * 1024u || pb_dev_label_ws_occupancy(32 * (nc + 1), smem, &occ) != 0) occ = 0;
+        cudaGetLastError();
+        t->occ_ws[i] = occ;
+    }
+    return t->occ_ws[i];
+}
+
+static uint64_t passes_lanes(const pose_hbm_topo_t *t, uint64_t lanes)
+{
+    uint64_t passes = 0;
+    for (uint32_t k = 0; k < t->nw; k++) passes += t->wcnt[k] * ((t->wval[k] + lanes - 1) / lanes);
+    return passes;
+}
+
 static int pipe_occupancy(pose_hbm_topo_t *t, uint32_t T, uint32_t G)
 {
     int ti = __builtin_ctz(T), gi = G == 1 ? 0 : 1;
@@ -177,6 +210,7 @@ static int make_plan(const pose_hbm_topo_t *ct, uint64_t nunits, const pose_b200
     best->cost = -1;
     for (int kernel = 1; kernel <= 2; kernel++) {
         if (want && want != kernel) continue;
+        if (want == 0 && kernel == 2 && t->d_recs2) continue; /* superseded by the warp-specialised kernel */
         if (kernel == 2 && !t->d_recs2) continue;
         for (uint32_t T = kernel == 2 ? 4 : 1; T <= 16; T <<= 1) {
             if (hint && hint->team_warps && hint->team_warps != T) continue;
@@ -216,6 +250,35 @@ static int make_plan(const pose_hbm_topo_t *ct, uint64_t nunits, const pose_b200
                     best->fma = kernel == 1 && alu >= lat; /* ALU-bound: move adds to the FMA pipe */
                 }
             }
+        }
+    }
+    /* warp-specialised kernel: one chunk copy per CTA, NC hashing warps */
+    for (uint32_t nc = 7; nc <= 15 && t->d_recs2 && (!want || want == 3); nc += 8) {
+        if (hint && hint->team_warps && hint->team_warps != nc) continue;
+        if (hint && hint->units_per_team > 1) continue;
+        int occ = ws_occupancy(t, nc);
+        if (occ <= 0) continue;
+        uint64_t team_scratch = (uint64_t)(t->view2.gpool ? t->view2.gpool : 1) * 32;
+        uint64_t batches = nunits;
+        uint64_t cap = (uint64_t)t->sms * occ;
+        uint64_t memcap = budget / team_scratch;
+        uint64_t R = cap < memcap ? cap : memcap;
+        if (R > batches) R = batches;
+        if (hint && hint->max_teams && R > hint->max_teams) R = hint->max_teams;
+        if (R == 0) continue;
+        uint64_t waves = (batches + R - 1) / R;
+        uint64_t passes = passes_lanes(t, 32ull * nc);
+        double lat = (double)t->L * model_ws_latency() + (double)(passes - t->L) * t_lat;
+        double teams_sm = (double)((R + t->sms - 1) / t->sms);
+        double alu = teams_sm * (double)t->S * item_instr / lanes_clk;
+        double cost = (double)waves * (lat > alu ? lat : alu);
+        uint64_t sbytes = R * team_scratch;
+        if (sbytes > budget) continue;
+        if (best->cost < 0 || cost < best->cost * 0.999) {
+            best->T = nc; best->G = 1; best->teams = (uint32_t)R;
+            best->grid = (uint32_t)R; best->cta = 32 * (nc + 1);
+            best->team_scratch = team_scratch; best->scratch_bytes = sbytes;
+            best->cost = cost; best->kernel = 3; best->smem = ws_smem_bytes(t, nc); best->fma = 0;
         }
     }
     return best->cost < 0 ? -1 : 0;
@@ -391,6 +454,7 @@ pose_hbm_topo_t *pose_b200_topo_build(uint32_t chunk_blocks, int with_cv0_table)
         t->view2.retained = h.retained; t->view2.csm = h.csm; t->view2.gpool = h.gpool2;
         memcpy(t->view2.desc, t->view.desc, sizeof(t->view2.desc));
         memset(t->occ_pipe, 0xFF, sizeof(t->occ_pipe));
+        memset(t->occ_ws, 0xFF, sizeof(t->occ_ws));
     }
     pb_topo_host_free(&h);
     return t;
@@ -455,9 +519,12 @@ int pose_b200_plan(const pose_hbm_topo_t *t, uint64_t super_chunks, const pose_b
     return 0;
 }
 
-int pose_b200_topo_label(const pose_hbm_topo_t *ct, const uint8_t *session_seed, size_t seed_len,
-                         void *hbm_dev_ptr, size_t hbm_len, uint64_t rbo,
-                         const pose_b200_sched_t *sched, pose_b200_stats_t *stats)
+/* The labeling call.  Chunk seeds come either from the session seed (derived
+ * per super-chunk from its absolute position), or, when raw_seeds is set, are
+ * taken as given: raw_seeds holds 32 bytes per super-chunk of the buffer. */
+static int topo_label_core(const pose_hbm_topo_t *ct, const uint8_t *session_seed, size_t seed_len,
+                           const uint8_t *raw_seeds, void *hbm_dev_ptr, size_t hbm_len, uint64_t rbo,
+                           const pose_b200_sched_t *sched, pose_b200_stats_t *stats)
 {
     pose_hbm_topo_t *t = (pose_hbm_topo_t *)ct; /* workspace is mutable state */
     if (stats) memset(stats, 0, sizeof(*stats));
@@ -465,15 +532,19 @@ int pose_b200_topo_label(const pose_hbm_topo_t *ct, const uint8_t *session_seed,
     uint64_t num_super = hbm_len / t->super_bytes;
     if (num_super == 0) return 0; /* smaller than one super-chunk: nothing to label */
     if (!hbm_dev_ptr) { set_err("pose_graph_hbm_topo_label: NULL buffer"); return -1; }
-    if (!session_seed && seed_len) { set_err("pose_graph_hbm_topo_label: NULL seed"); return -1; }
-    if (sched && ((sched->team_warps && (!is_pow2(sched->team_warps) || sched->team_warps > 16)) ||
+    if (!raw_seeds && !session_seed && seed_len) { set_err("pose_graph_hbm_topo_label: NULL seed"); return -1; }
+    if (sched && sched->kernel == 3 && sched->team_warps && sched->team_warps != 7 && sched->team_warps != 15) {
+        set_err("pose_b200_topo_label: the warp-specialised kernel takes 7 or 15 hashing warps");
+        return -1;
+    }
+    if (sched && sched->kernel != 3 && ((sched->team_warps && (!is_pow2(sched->team_warps) || sched->team_warps > 16)) ||
                   (sched->units_per_team &&
                    (!is_pow2(sched->units_per_team) || sched->units_per_team > 32)))) {
         set_err("pose_b200_topo_label: schedule must use powers of two (T <= 16, G <= 32)");
         return -1;
     }
-    if (sched && sched->kernel > 2) {
-        set_err("pose_b200_topo_label: kernel must be 0 (automatic), 1 or 2");
+    if (sched && sched->kernel > 3) {
+        set_err("pose_b200_topo_label: kernel must be 0 (automatic), 1, 2 or 3");
         return -1;
     }
     int prev = -1, rc = -1;
@@ -508,7 +579,7 @@ int pose_b200_topo_label(const pose_hbm_topo_t *ct, const uint8_t *session_seed,
             set_err("pose_graph_hbm_topo_label: seed buffer alloc failed");
             goto out;
         }
-        const int dev_seeds = seed_len <= PB_DEVICE_SEED_MAX;
+        const int dev_seeds = !raw_seeds && seed_len <= PB_DEVICE_SEED_MAX;
         if (dev_seeds && seed_len) {
             uint64_t have = t->sess_alloc;
             if (grow((void **)&t->d_sess, &have, seed_len, 1) != 0) {
@@ -524,7 +595,11 @@ int pose_b200_topo_label(const pose_hbm_topo_t *ct, const uint8_t *session_seed,
         uint32_t launches = 0;
         for (uint64_t first = 0; first < num_super; first += per_launch) {
             uint64_t n = num_super - first < per_launch ? num_super - first : per_launch;
-            if (dev_seeds) {
+            if (raw_seeds) {
+                CK(cudaMemcpyAsync(t->d_seeds, raw_seeds + 32 * first, n * 32, cudaMemcpyHostToDevice, t->stream),
+                   "seed upload");
+                CK(cudaStreamSynchronize(t->stream), "seed upload");
+            } else if (dev_seeds) {
                 if (pb_dev_chunk_seeds(t->d_sess, (uint32_t)seed_len, rbo, t->cb, (uint32_t)n, first,
                                        t->d_seeds, t->stream) != 0) {
                     set_err("pose_graph_hbm_topo_label: chunk-seed kernel failed");
@@ -564,7 +639,7 @@ int pose_b200_topo_label(const pose_hbm_topo_t *ct, const uint8_t *session_seed,
             { const char *e = getenv("POSE_B200_FMA_ADDS"); if (e && e[0]) p.fma_adds = (uint32_t)atoi(e); }
             CK(cudaEventRecord(t->ev[1], t->stream), "event");
             int lrc;
-            if (plan.kernel == 2) {
+            if (plan.kernel == 2 || plan.kernel == 3) {
                 pb_pipe_params_t pp;
                 memset(&pp, 0, sizeof(pp));
                 pp.topo = t->view2;
@@ -573,7 +648,8 @@ int pose_b200_topo_label(const pose_hbm_topo_t *ct, const uint8_t *session_seed,
                 pp.team_scratch_bytes = plan.team_scratch; pp.nunits = p.nunits;
                 pp.copies_log2 = p.copies_log2; pp.g_log2 = p.g_log2; pp.team_warps = p.team_warps;
                 pp.nbatches = p.nbatches; pp.queue = p.queue;
-                lrc = pb_dev_label_pipe(&pp, plan.grid, plan.cta, plan.smem, t->stream);
+                lrc = plan.kernel == 2 ? pb_dev_label_pipe(&pp, plan.grid, plan.cta, plan.smem, t->stream)
+                                       : pb_dev_label_ws(&pp, plan.grid, plan.cta, plan.smem, t->stream);
             } else {
                 lrc = pb_dev_label(&p, plan.grid, plan.cta, t->stream);
             }
@@ -586,7 +662,7 @@ int pose_b200_topo_label(const pose_hbm_topo_t *ct, const uint8_t *session_seed,
             launches++;
             CK(cudaEventSynchronize(t->ev[2]), "label kernel");
             float ms = 0;
-            cudaEventElapsedTime(&ms, t->ev[1], t->ev[2]);
+            if (cudaEventElapsedTime(&ms, t->ev[1], t->ev[2]) != cudaSuccess) { cudaGetLastError(); ms = 0; }
             kms += ms;
         }
         /* scratch and seeds never outlive the call (the reference zeroes its
@@ -596,7 +672,7 @@ int pose_b200_topo_label(const pose_hbm_topo_t *ct, const uint8_t *session_seed,
         CK(cudaEventRecord(t->ev[3], t->stream), "event");
         CK(cudaStreamSynchronize(t->stream), "label");
         float tms = 0;
-        cudaEventElapsedTime(&tms, t->ev[0], t->ev[3]);
+        if (cudaEventElapsedTime(&tms, t->ev[0], t->ev[3]) != cudaSuccess) { cudaGetLastError(); tms = 0; }
         double elapsed = now_sec() - t0;
         if (stats) {
             stats->kernel_ms = kms;
@@ -628,6 +704,20 @@ out:
     }
     if (prev >= 0 && prev != t->device) cudaSetDevice(prev);
     return rc;
+}
+
+int pose_b200_topo_label(const pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
+                         void *hbm_dev_ptr, size_t hbm_len, uint64_t rbo,
+                         const pose_b200_sched_t *sched, pose_b200_stats_t *stats)
+{
+    return topo_label_core(topo, session_seed, seed_len, NULL, hbm_dev_ptr, hbm_len, rbo, sched, stats);
+}
+
+int pb_topo_label_raw(const pose_hbm_topo_t *topo, const uint8_t *chunk_seeds, void *hbm_dev_ptr,
+                      size_t hbm_len, const pose_b200_sched_t *sched, pose_b200_stats_t *stats)
+{
+    if (!chunk_seeds) { set_err("pose_b200: NULL chunk seeds"); return -1; }
+    return topo_label_core(topo, NULL, 0, chunk_seeds, hbm_dev_ptr, hbm_len, 0, sched, stats);
 }
 
 int pose_graph_hbm_topo_label(const pose_hbm_topo_t *topo, const uint8_t *session_seed,
@@ -763,7 +853,21 @@ int pb_topo_internal(const pose_hbm_topo_t *t, pb_topo_internal_t *out)
     out->super_bytes = t->super_bytes;
     out->view = t->view;
     out->stream = t->stream;
+    out->sms = t->sms;
     return 0;
+}
+
+uint64_t pb_topo_passes(const pose_hbm_topo_t *t, uint32_t T, uint32_t G)
+{
+    return t ? passes_for(t, T, G) : 0;
+}
+
+uint64_t pb_topo_scratch_budget(const pose_hbm_topo_t *t, uint64_t cap)
+{
+    pose_b200_sched_t s;
+    memset(&s, 0, sizeof(s));
+    s.scratch_cap_bytes = cap;
+    return scratch_budget(t, &s);
 }
 
 int pb_plan_for_budget(const pose_hbm_topo_t *t, uint64_t nunits, uint64_t budget, pb_plan_out_t *out)

@@ -1,0 +1,457 @@
+/*
+ * label_batch.c — batched labeling (C11 host side of k_label_multi).
+ *
+ * Many requests — each one session seed, one topology (chunk_blocks), one
+ * device buffer and one region_block_offset, with the semantics of a
+ * pose_graph_hbm_topo_label call — run in one persistent launch:
+ *
+ *   - every super-chunk of every request contributes its two chunk copies
+ *     (units); its chunk seed is derived on the device from a seed job
+ *     (session seed in a packed blob, chunk index (rbo + j*cb)/cb);
+ *   - units of one topology are grouped G at a time into batches that a team
+ *     of T warps runs in lockstep.  A warp with no node in a level skips it,
+ *     so the ALU work of a batch is sum over levels of ceil(G*w/32) warp
+ *     passes whatever T is, while its chain is sum of ceil(G*w/(32T)): wide
+ *     teams shorten the deep topologies' chains for free, and a shallow
+ *     topology packs G units while its chain stays under the deepest one's;
+ *   - T and the packing rule are chosen by an estimate of the makespan (the
+ *     longest chain against the ALU time of all warp passes);
+ *   - batches are queued longest first (by passes), so the deep topologies
+ *     start at once and the short ones fill in behind them;
+ *   - seed derivation, queue reset, the labeling kernel and the scratch
+ *     zeroing are captured once into a CUDA graph and replayed.
+ */
+#include "batch_internal.h"
+#include "kernels.h"
+#include "topo_internal.h"
+#include "pose_b200.h"
+
+#include <cuda_runtime_api.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+struct pose_b200_batch {
+    int device;
+    cudaStream_t stream;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    cudaEvent_t ev[4];
+    void *d_topos, *d_batches, *d_units, *d_jobs, *d_blob, *d_seeds, *d_scratch, *d_queue;
+    uint64_t scratch_bytes, nodes, super_chunks, units;
+    uint32_t nbatches, teams, T, Gmax, fma, cv0;
+};
+
+typedef struct {
+    uint64_t cost;
+    pb_mbatch_t b;
+} batch_sort_t;
+
+static int cmp_batch(const void *a, const void *b)
+{
+    uint64_t x = ((const batch_sort_t *)a)->cost, y = ((const batch_sort_t *)b)->cost;
+    return x < y ? 1 : x > y ? -1 : 0;
+}
+
+static void batch_free(pose_b200_batch_t *b)
+{
+    if (!b) return;
+    if (b->stream) {
+        if (b->d_scratch) cudaMemsetAsync(b->d_scratch, 0, b->scratch_bytes, b->stream);
+        if (b->d_seeds) cudaMemsetAsync(b->d_seeds, 0, (size_t)b->super_chunks * 32, b->stream);
+        cudaStreamSynchronize(b->stream);
+    }
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    cudaFree(b->d_topos); cudaFree(b->d_batches); cudaFree(b->d_units); cudaFree(b->d_jobs);
+    cudaFree(b->d_blob); cudaFree(b->d_seeds); cudaFree(b->d_scratch); cudaFree(b->d_queue);
+    for (int i = 0; i < 4; i++) if (b->ev[i]) cudaEventDestroy(b->ev[i]);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    free(b);
+}
+
+void pose_b200_batch_destroy(pose_b200_batch_t *b) { batch_free(b); }
+
+#define BK(call, what)                                                                    \
+    do {                                                                                  \
+        if ((call) != cudaSuccess) {                                                      \
+            fprintf(stderr, "pose_b200_batch_create: %s: %s\n", what,                     \
+                    cudaGetErrorString(cudaGetLastError()));                              \
+            goto fail;                                                                    \
+        }                                                                                 \
+    } while (0)
+
+void pb_plan_free(pb_plan_tables_t *p)
+{
+    if (!p) return;
+    free(p->views);
+    free(p->units);
+    free(p->unit_req);
+    free(p->jobs);
+    free(p->batches);
+    memset(p, 0, sizeof(*p));
+}
+
+int pb_plan_requests(const pb_req_t *reqs, size_t n, uint32_t T, uint32_t gcap, double eff_min,
+                     pb_plan_tables_t *out)
+{
+    memset(out, 0, sizeof(*out));
+    const pose_hbm_topo_t **topo_list = (const pose_hbm_topo_t **)calloc(n ? n : 1, sizeof(*topo_list));
+    pb_topo_internal_t *ti = (pb_topo_internal_t *)calloc(n ? n : 1, sizeof(*ti));
+    uint32_t *G = NULL, *nunits_t = NULL, *ucount = NULL;
+    uint64_t *ufirst = NULL;
+    batch_sort_t *bs = NULL;
+    size_t ntopo = 0;
+    uint64_t njobs = 0, total_units = 0;
+    int dev = -1, rc = -1;
+    if (!topo_list || !ti) goto done;
+    cudaGetDevice(&dev);
+    for (size_t i = 0; i < n; i++) {
+        const pb_req_t *r = &reqs[i];
+        pb_topo_internal_t x;
+        if (pb_topo_internal(r->topo, &x) != 0) { fprintf(stderr, "pose_b200: request %zu has no topology\n", i); goto done; }
+        if (x.device != dev) { fprintf(stderr, "pose_b200: request %zu: topology of another device\n", i); goto done; }
+        uint64_t ns = r->len / x.super_bytes;
+        if (ns && !r->dev_ptr) { fprintf(stderr, "pose_b200: request %zu: NULL buffer\n", i); goto done; }
+        size_t k = 0;
+        while (k < ntopo && topo_list[k] != r->topo) k++;
+        if (k == ntopo) { topo_list[ntopo] = r->topo; ti[ntopo] = x; ntopo++; }
+        njobs += ns;
+        total_units += ns * x.copies;
+    }
+    if (total_units > 0xFFFFFFFFull) { fprintf(stderr, "pose_b200: too many chunk copies\n"); goto done; }
+    out->ntopo = ntopo;
+    out->nunits = total_units;
+    out->njobs = njobs;
+    out->sms = ntopo ? (uint32_t)ti[0].sms : 0;
+    out->all_cv0 = 1;
+    G = (uint32_t *)calloc(ntopo + 1, 4);
+    nunits_t = (uint32_t *)calloc(ntopo + 1, 4);
+    ufirst = (uint64_t *)calloc(ntopo + 1, 8);
+    ucount = (uint32_t *)calloc(ntopo + 1, 4);
+    out->views = (pb_topo_view_t *)calloc(ntopo + 1, sizeof(pb_topo_view_t));
+    out->units = (pb_munit_t *)calloc(total_units + 1, sizeof(pb_munit_t));
+    out->unit_req = (uint32_t *)calloc(total_units + 1, sizeof(uint32_t));
+    out->jobs = (pb_seedjob_t *)calloc(njobs + 1, sizeof(pb_seedjob_t));
+    if (!G || !nunits_t || !ufirst || !ucount || !out->views || !out->units || !out->unit_req || !out->jobs) goto done;
+    for (size_t i = 0; i < n; i++) {
+        size_t k = 0;
+        while (topo_list[k] != reqs[i].topo) k++;
+        nunits_t[k] += (uint32_t)((reqs[i].len / ti[k].super_bytes) * ti[k].copies);
+    }
+    {
+        uint64_t acc = 0;
+        for (size_t k = 0; k < ntopo; k++) {
+            ufirst[k] = acc;
+            acc += nunits_t[k];
+            out->views[k] = ti[k].view;
+            if (!ti[k].view.cv0) out->all_cv0 = 0;
+        }
+    }
+    {
+        uint64_t job = 0;
+        for (size_t i = 0; i < n; i++) {
+            const pb_req_t *r = &reqs[i];
+            size_t k = 0;
+            while (topo_list[k] != r->topo) k++;
+            uint64_t ns = r->len / ti[k].super_bytes;
+            for (uint64_t j = 0; j < ns; j++, job++) {
+                out->jobs[job].chunk_index = (r->rbo + j * (uint64_t)ti[k].cb) / ti[k].cb;
+                out->jobs[job].seed_off = r->seed_off;
+                out->jobs[job].seed_len = r->seed_len;
+                for (uint32_t c = 0; c < ti[k].copies; c++) {
+                    out->unit_req[ufirst[k] + ucount[k]] = (uint32_t)i;
+                    pb_munit_t *u = &out->units[ufirst[k] + ucount[k]++];
+                    u->out = (uint64_t)(uintptr_t)r->dev_ptr + j * ti[k].super_bytes;
+                    u->seed = (uint32_t)job;
+                    u->copy = c;
+                }
+            }
+        }
+    }
+    /* G per topology.  eff_min > 0: the smallest power of two whose lane
+     * efficiency G*S / (passes * 32T) reaches eff_min.  eff_min <= 0: pack
+     * units as long as the batch's chain of passes stays within the longest
+     * chain of the launch at G = 1 (the deepest topology sets the makespan;
+     * packing shallower ones costs no time and fills partial warps). */
+    uint64_t chain_cap = 0;
+    for (size_t k = 0; k < ntopo; k++) {
+        uint64_t p1 = pb_topo_passes(topo_list[k], T, 1);
+        if (p1 > chain_cap) chain_cap = p1;
+    }
+    uint64_t nb = 0;
+    for (size_t k = 0; k < ntopo; k++) {
+        uint32_t g = 1;
+        while (g * 2 <= gcap && g * 2 <= 32 * T && g < nunits_t[k]) {
+            if (eff_min > 0) {
+                uint64_t passes = pb_topo_passes(topo_list[k], T, g);
+                double eff = (double)g * ti[k].view.S / ((double)passes * 32.0 * T);
+                if (eff >= eff_min) break;
+            } else if (pb_topo_passes(topo_list[k], T, g * 2) > chain_cap) {
+                break;
+            }
+            g *= 2;
+        }
+        G[k] = g;
+        if (g > out->Gmax) out->Gmax = g;
+        nb += (nunits_t[k] + g - 1) / g;
+        uint64_t ts = (uint64_t)g * ti[k].view.pool * 32;
+        if (ts > out->team_scratch) out->team_scratch = ts;
+        out->nodes += (uint64_t)nunits_t[k] * ti[k].view.S;
+    }
+    bs = (batch_sort_t *)calloc(nb + 1, sizeof(*bs));
+    out->batches = (pb_mbatch_t *)calloc(nb + 1, sizeof(pb_mbatch_t));
+    if (!bs || !out->batches) goto done;
+    {
+        uint64_t q = 0;
+        for (size_t k = 0; k < ntopo; k++) {
+            uint64_t passes = pb_topo_passes(topo_list[k], T, G[k]);
+            for (uint32_t f = 0; f < nunits_t[k]; f += G[k]) {
+                bs[q].b.topo = (uint32_t)k;
+                bs[q].b.first_unit = (uint32_t)(ufirst[k] + f);
+                bs[q].b.count = nunits_t[k] - f < G[k] ? nunits_t[k] - f : G[k];
+                bs[q].b.glog = (uint32_t)__builtin_ctz(G[k]);
+                bs[q].cost = passes;
+                if (passes > out->max_chain) out->max_chain = passes;
+                q++;
+            }
+        }
+        qsort(bs, nb, sizeof(*bs), cmp_batch);
+        for (uint64_t i = 0; i < nb; i++) out->batches[i] = bs[i].b;
+    }
+    out->nbatches = nb;
+    /* warps of a team that have no node of a level skip it, so the ALU work
+     * of a batch is its one-warp pass count: sum over levels of ceil(G*w/32) */
+    out->warp_passes = 0;
+    for (size_t k = 0; k < ntopo; k++)
+        out->warp_passes += (double)((nunits_t[k] + G[k] - 1) / G[k]) * (double)pb_topo_passes(topo_list[k], 1, G[k]);
+    rc = 0;
+done:
+    free(topo_list); free(ti); free(G); free(nunits_t); free(ufirst); free(ucount); free(bs);
+    if (rc != 0) pb_plan_free(out);
+    return rc;
+}
+
+double pb_plan_makespan(const pb_plan_tables_t *p, uint32_t T, uint64_t R)
+{
+    /* per pass: ~3500 clocks when latency-bound; ALU: a warp-pass is 32 lanes
+     * x 2 compressions (~1400 operations a lane) at ~72 lane-operations per
+     * clock per SM */
+    (void)T;
+    double chain = (double)p->max_chain * 3500.0;
+    double sms = p->sms ? p->sms : 148;
+    double alu = p->warp_passes * 32.0 * 1400.0 / (72.0 * sms);
+    double waves = R && p->nbatches > R ? 1.0 + (double)(p->nbatches - R) / (double)R * 0.5 : 1.0;
+    return (chain > alu ? chain : alu) * waves;
+}
+
+int pb_plan_choose(const pb_req_t *pr, size_t n, const pose_b200_sched_t *sched, uint32_t *T_out, double *eff_out)
+{
+    /* the lowest estimated makespan over the team sizes and packing rules
+     * (chain-bounded, or a lane-efficiency target) the caller left open */
+    const uint32_t gcap = sched && sched->units_per_team ? sched->units_per_team : 32;
+    const uint32_t t_lo = sched && sched->team_warps ? sched->team_warps : 1;
+    const uint32_t t_hi = sched && sched->team_warps ? sched->team_warps : 8;
+    double rules[4] = {0.0, 0.5, 0.7, 0.85};
+    int nrules = 4;
+    if (sched && sched->lane_efficiency) {
+        rules[0] = sched->lane_efficiency / 100.0;
+        nrules = 1;
+    }
+    double best = -1;
+    for (uint32_t tT = t_lo; tT <= t_hi; tT <<= 1) {
+        for (int e = 0; e < nrules; e++) {
+            pb_plan_tables_t cand;
+            if (pb_plan_requests(pr, n, tT, gcap, rules[e], &cand) != 0) return -1;
+            double ms = pb_plan_makespan(&cand, tT, (uint64_t)cand.sms * 32 / tT);
+            if (best < 0 || ms < best) { best = ms; *T_out = tT; *eff_out = rules[e]; }
+            pb_plan_free(&cand);
+        }
+    }
+    return 0;
+}
+
+pose_b200_batch_t *pose_b200_batch_create(const pose_b200_request_t *reqs, size_t n,
+                                          const pose_b200_sched_t *sched)
+{
+    pose_b200_batch_t *b = NULL;
+    pb_req_t *pr = NULL;
+    uint8_t *blob = NULL;
+    pb_plan_tables_t pl;
+    memset(&pl, 0, sizeof(pl));
+    size_t blob_len = 0;
+    int dev = -1;
+
+    if (!reqs || n == 0) { fprintf(stderr, "pose_b200_batch_create: no requests\n"); return NULL; }
+    if (sched && sched->team_warps && sched->team_warps != 1 && sched->team_warps != 2 && sched->team_warps != 4 &&
+        sched->team_warps != 8) {
+        fprintf(stderr, "pose_b200_batch_create: team_warps must be 1, 2, 4 or 8\n");
+        return NULL;
+    }
+    for (size_t i = 0; i < n; i++) {
+        if (!reqs[i].session_seed && reqs[i].seed_len) { fprintf(stderr, "pose_b200_batch_create: request %zu: NULL seed\n", i); return NULL; }
+        if (reqs[i].seed_len > 1016) { fprintf(stderr, "pose_b200_batch_create: request %zu: seed longer than 1016 bytes\n", i); return NULL; }
+        blob_len += reqs[i].seed_len;
+    }
+    pr = (pb_req_t *)calloc(n, sizeof(*pr));
+    blob = (uint8_t *)malloc(blob_len ? blob_len : 1);
+    if (!pr || !blob) goto fail_host;
+    {
+        uint64_t off = 0;
+        for (size_t i = 0; i < n; i++) {
+            pr[i].topo = reqs[i].topo;
+            pr[i].dev_ptr = reqs[i].hbm_dev_ptr;
+            pr[i].len = reqs[i].hbm_len;
+            pr[i].rbo = reqs[i].region_block_offset;
+            pr[i].seed_off = (uint32_t)off;
+            pr[i].seed_len = (uint32_t)reqs[i].seed_len;
+            if (reqs[i].seed_len) memcpy(blob + off, reqs[i].session_seed, reqs[i].seed_len);
+            off += reqs[i].seed_len;
+        }
+    }
+    const uint32_t gcap = sched && sched->units_per_team ? sched->units_per_team : 32;
+    uint32_t T = 4;
+    double eff = 0.0;
+    if (pb_plan_choose(pr, n, sched, &T, &eff) != 0) goto fail_host;
+    if (pb_plan_requests(pr, n, T, gcap, eff, &pl) != 0) goto fail_host;
+    if (pl.nunits == 0) { fprintf(stderr, "pose_b200_batch_create: no super-chunk to label\n"); goto fail_host; }
+    cudaGetDevice(&dev);
+
+    b = (pose_b200_batch_t *)calloc(1, sizeof(*b));
+    if (!b) goto fail_host;
+    b->device = dev;
+    b->T = T;
+    b->nbatches = (uint32_t)pl.nbatches;
+    b->units = pl.nunits;
+    b->super_chunks = pl.njobs;
+    b->nodes = pl.nodes;
+    b->Gmax = pl.Gmax;
+    b->cv0 = pl.all_cv0;
+    {
+        const uint32_t cta = 256, tpc = cta / (32 * T);
+        int occ = 0;
+        BK(pb_dev_label_multi_occupancy(cta, &occ) == 0 ? cudaSuccess : cudaErrorUnknown, "occupancy");
+        uint64_t cap = (uint64_t)pl.sms * (occ > 0 ? occ : 1) * tpc;
+        uint64_t budget = pb_topo_scratch_budget(reqs[0].topo, sched ? sched->scratch_cap_bytes : 0);
+        uint64_t R = budget / pl.team_scratch;
+        if (R > cap) R = cap;
+        if (R > pl.nbatches) R = pl.nbatches;
+        if (sched && sched->max_teams && R > sched->max_teams) R = sched->max_teams;
+        if (R == 0) {
+            fprintf(stderr, "pose_b200_batch_create: one team needs %llu bytes of scratch, over the budget\n",
+                    (unsigned long long)pl.team_scratch);
+            goto fail;
+        }
+        /* CTAs of up to tpc teams; every team of every CTA has its scratch */
+        const uint32_t ctpc = R < tpc ? (uint32_t)R : tpc;
+        const uint32_t grid = (uint32_t)(R / ctpc);
+        R = (uint64_t)grid * ctpc;
+        const uint32_t cta_threads = 32 * T * ctpc;
+        b->teams = (uint32_t)R;
+        b->fma = (double)R * T / pl.sms >= 8.0;
+        b->scratch_bytes = R * pl.team_scratch;
+
+        BK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream");
+        for (int i = 0; i < 4; i++) BK(cudaEventCreate(&b->ev[i]), "event");
+        BK(cudaMalloc(&b->d_topos, pl.ntopo * sizeof(pb_topo_view_t)), "alloc");
+        BK(cudaMalloc(&b->d_batches, pl.nbatches * sizeof(pb_mbatch_t)), "alloc");
+        BK(cudaMalloc(&b->d_units, pl.nunits * sizeof(pb_munit_t)), "alloc");
+        BK(cudaMalloc(&b->d_jobs, pl.njobs * sizeof(pb_seedjob_t)), "alloc");
+        BK(cudaMalloc(&b->d_blob, blob_len ? blob_len : 1), "alloc");
+        BK(cudaMalloc(&b->d_seeds, pl.njobs * 32), "alloc");
+        BK(cudaMalloc(&b->d_scratch, b->scratch_bytes), "scratch alloc");
+        BK(cudaMalloc(&b->d_queue, 64), "alloc");
+        BK(cudaMemcpyAsync(b->d_topos, pl.views, pl.ntopo * sizeof(pb_topo_view_t), cudaMemcpyHostToDevice, b->stream), "upload");
+        BK(cudaMemcpyAsync(b->d_batches, pl.batches, pl.nbatches * sizeof(pb_mbatch_t), cudaMemcpyHostToDevice, b->stream), "upload");
+        BK(cudaMemcpyAsync(b->d_units, pl.units, pl.nunits * sizeof(pb_munit_t), cudaMemcpyHostToDevice, b->stream), "upload");
+        BK(cudaMemcpyAsync(b->d_jobs, pl.jobs, pl.njobs * sizeof(pb_seedjob_t), cudaMemcpyHostToDevice, b->stream), "upload");
+        if (blob_len) BK(cudaMemcpyAsync(b->d_blob, blob, blob_len, cudaMemcpyHostToDevice, b->stream), "upload");
+        BK(cudaStreamSynchronize(b->stream), "upload");
+
+        pb_multi_params_t p;
+        memset(&p, 0, sizeof(p));
+        p.topos = (const pb_topo_view_t *)b->d_topos;
+        p.batches = (const pb_mbatch_t *)b->d_batches;
+        p.units = (const pb_munit_t *)b->d_units;
+        p.seeds = (const uint32_t *)b->d_seeds;
+        p.scratch = (uint8_t *)b->d_scratch;
+        p.team_scratch_bytes = pl.team_scratch;
+        p.nbatches = (uint32_t)pl.nbatches;
+        p.team_warps = T;
+        p.queue = (unsigned int *)b->d_queue;
+        p.fma_adds = b->fma;
+        p.one = 1;
+        BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "capture");
+        int crc = pb_dev_seed_jobs(b->d_jobs, (uint32_t)pl.njobs, (const uint8_t *)b->d_blob, (uint32_t *)b->d_seeds,
+                                   b->stream);
+        if (crc == 0) crc = cudaMemsetAsync(b->d_queue, 0, 64, b->stream) == cudaSuccess ? 0 : -1;
+        if (crc == 0) crc = cudaEventRecord(b->ev[1], b->stream) == cudaSuccess ? 0 : -1;
+        if (crc == 0) crc = pb_dev_label_multi(&p, grid, cta_threads, b->stream);
+        if (crc == 0) crc = cudaEventRecord(b->ev[2], b->stream) == cudaSuccess ? 0 : -1;
+        if (crc == 0) crc = cudaMemsetAsync(b->d_scratch, 0, b->scratch_bytes, b->stream) == cudaSuccess ? 0 : -1;
+        cudaError_t ce = cudaStreamEndCapture(b->stream, &b->graph);
+        if (crc != 0 || ce != cudaSuccess) {
+            fprintf(stderr, "pose_b200_batch_create: graph capture failed: %s\n",
+                    cudaGetErrorString(ce != cudaSuccess ? ce : cudaGetLastError()));
+            goto fail;
+        }
+        BK(cudaGraphInstantiate(&b->exec, b->graph, 0), "graph instantiate");
+    }
+    free(pr); free(blob); pb_plan_free(&pl);
+    return b;
+fail:
+    batch_free(b);
+    b = NULL;
+fail_host:
+    cudaGetLastError();
+    free(pr); free(blob); pb_plan_free(&pl);
+    return NULL;
+}
+
+int pose_b200_batch_run(pose_b200_batch_t *b, pose_b200_stats_t *stats)
+{
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (!b) return -1;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != b->device) cudaSetDevice(b->device);
+    int rc = -1;
+    if (cudaEventRecord(b->ev[0], b->stream) != cudaSuccess) goto out;
+    if (cudaGraphLaunch(b->exec, b->stream) != cudaSuccess) goto out;
+    if (cudaEventRecord(b->ev[3], b->stream) != cudaSuccess) goto out;
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) goto out;
+    rc = 0;
+    if (stats) {
+        float k = 0, t = 0;
+        if (cudaEventElapsedTime(&t, b->ev[0], b->ev[3]) != cudaSuccess) { cudaGetLastError(); t = 0; }
+        /* the kernel's own events are nodes of the graph; where the driver
+         * does not time them, report the whole replay */
+        if (cudaEventElapsedTime(&k, b->ev[1], b->ev[2]) != cudaSuccess || k <= 0) { cudaGetLastError(); k = t; }
+        stats->kernel_ms = k;
+        stats->total_ms = t;
+        stats->super_chunks = b->super_chunks;
+        stats->units = b->units;
+        stats->nodes = b->nodes;
+        stats->scratch_bytes = b->scratch_bytes;
+        stats->team_warps = b->T;
+        stats->units_per_team = b->Gmax;
+        stats->teams = b->teams;
+        stats->kernel_launches = 2; /* seeds + labeling */
+        stats->used_cv0_table = b->cv0;
+        stats->kernel = 4;
+    }
+out:
+    if (rc != 0) fprintf(stderr, "pose_b200_batch_run: CUDA error: %s\n", cudaGetErrorString(cudaGetLastError()));
+    if (prev >= 0 && prev != b->device) cudaSetDevice(prev);
+    return rc;
+}
+
+int pose_b200_label_batch(const pose_b200_request_t *reqs, size_t n, const pose_b200_sched_t *sched,
+                          pose_b200_stats_t *stats)
+{
+    pose_b200_batch_t *b = pose_b200_batch_create(reqs, n, sched);
+    if (!b) return -1;
+    int rc = pose_b200_batch_run(b, stats);
+    pose_b200_batch_destroy(b);
+    return rc;
+}

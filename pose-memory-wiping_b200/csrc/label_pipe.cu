@@ -264,6 +264,7 @@ extern "C" int pb_dev_label_pipe(const pb_pipe_params_t *params, uint32_t grid, 
     if (cudaFuncSetAttribute(pb::k_label_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem_bytes) != cudaSuccess)
         return -1;
+    cudaGetLastError(); /* report only this launch */
     pb::k_label_pipe<<<grid, cta_threads, smem_bytes, stream>>>(*params);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

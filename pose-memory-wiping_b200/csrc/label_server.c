@@ -1,0 +1,571 @@
+/*
+ * label_server.c — a continuous-batching labeling server (C11 + pthreads).
+ *
+ * Requests (topology, session, device buffer, region_block_offset — the
+ * arguments of pose_graph_hbm_topo_label with the session seed kept on the
+ * device) are submitted from any thread.  A dispatcher thread owns the GPU
+ * side:
+ *   - sessions: every session seed lives in one device blob; seed jobs of a
+ *     launch point into it (chunk seeds are derived on the device);
+ *   - admission: pending requests are taken, oldest first, into a "wave" as
+ *     soon as a wave slot (stream) is free and the scratch arena has room for
+ *     at least one team; a wave's teams are as many as the arena's free space,
+ *     the GPU's residency and the wave's batches allow;
+ *   - a wave is one persistent multi-topology launch (k_label_multi) on its
+ *     own stream with its own arena range; waves run concurrently, and a
+ *     wave's teams leave as its queue drains, so newly admitted work fills the
+ *     GPU behind it;
+ *   - completion, per request: when a team finishes a batch, each of its
+ *     units adds 1 to its request's counter in mapped host memory (after a
+ *     system-scope fence), and the dispatcher marks a request done as soon as
+ *     all its chunk copies are in, while the rest of its wave still runs;
+ *   - finished waves are reaped and their arena range is zeroed on the device
+ *     before it is reused.
+ * Every request's bytes are those of labelling it alone.
+ */
+#include "batch_internal.h"
+#include "kernels.h"
+#include "pose_b200.h"
+
+#include <cuda_runtime_api.h>
+#include <errno.h>
+#include <pthread.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#define PB_SERVER_MAX_WAVES 16
+
+typedef struct {
+    const pose_hbm_topo_t *topo;
+    void *dev_ptr;
+    size_t len;
+    uint64_t rbo;
+    int session;
+    int state; /* 0 pending, 1 running, 2 done, 3 failed */
+    double t_submit, t_start, t_done;
+} sreq_t;
+
+typedef struct {
+    int busy;
+    cudaStream_t stream;
+    cudaEvent_t done;
+    uint64_t arena_off, arena_len;
+    void *d_tables;
+    size_t tables_cap;
+    uint64_t *reqs;
+    uint32_t *need;            /* chunk copies of each request of the wave */
+    size_t nreqs, reqs_cap;
+    unsigned int *h_done;      /* mapped host counters, one per request */
+    unsigned int *d_done;
+    size_t done_cap;
+} wave_t;
+
+struct pose_b200_server {
+    int device, running;
+    pthread_t thread;
+    pthread_mutex_t mu;
+    pthread_cond_t cv;
+    /* sessions */
+    uint8_t *d_sessions;
+    size_t sess_bytes, sess_cap;
+    uint32_t *sess_off, *sess_len;
+    size_t nsess, sess_arr_cap;
+    /* requests */
+    sreq_t *reqs;
+    size_t nreqs, reqs_cap, next_pending;
+    /* scratch arena: free ranges */
+    uint8_t *d_arena;
+    uint64_t arena_bytes;
+    uint64_t free_off[2 * PB_SERVER_MAX_WAVES + 2], free_len[2 * PB_SERVER_MAX_WAVES + 2];
+    int nfree;
+    wave_t waves[PB_SERVER_MAX_WAVES];
+    uint32_t max_waves;
+    int occ;
+    uint64_t waves_launched;
+    double busy_ms;
+};
+
+static double now_ms(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return 1e3 * (double)ts.tv_sec + 1e-6 * (double)ts.tv_nsec;
+}
+
+/* first fit, keeping the free list sorted by offset */
+static int arena_take(pose_b200_server_t *s, uint64_t want, uint64_t *off)
+{
+    for (int i = 0; i < s->nfree; i++) {
+        if (s->free_len[i] >= want) {
+            *off = s->free_off[i];
+            s->free_off[i] += want;
+            s->free_len[i] -= want;
+            if (s->free_len[i] == 0) {
+                memmove(&s->free_off[i], &s->free_off[i + 1], (size_t)(s->nfree - i - 1) * 8);
+                memmove(&s->free_len[i], &s->free_len[i + 1], (size_t)(s->nfree - i - 1) * 8);
+                s->nfree--;
+            }
+            return 0;
+        }
+    }
+    return -1;
+}
+
+static uint64_t arena_largest(const pose_b200_server_t *s)
+{
+    uint64_t m = 0;
+    for (int i = 0; i < s->nfree; i++) if (s->free_len[i] > m) m = s->free_len[i];
+    return m;
+}
+
+static void arena_give(pose_b200_server_t *s, uint64_t off, uint64_t len)
+{
+    int i = 0;
+    while (i < s->nfree && s->free_off[i] < off) i++;
+    memmove(&s->free_off[i + 1], &s->free_off[i], (size_t)(s->nfree - i) * 8);
+    memmove(&s->free_len[i + 1], &s->free_len[i], (size_t)(s->nfree - i) * 8);
+    s->free_off[i] = off;
+    s->free_len[i] = len;
+    s->nfree++;
+    /* merge neighbours */
+    for (int k = 0; k + 1 < s->nfree;) {
+        if (s->free_off[k] + s->free_len[k] == s->free_off[k + 1]) {
+            s->free_len[k] += s->free_len[k + 1];
+            memmove(&s->free_off[k + 1], &s->free_off[k + 2], (size_t)(s->nfree - k - 2) * 8);
+            memmove(&s->free_len[k + 1], &s->free_len[k + 2], (size_t)(s->nfree - k - 2) * 8);
+            s->nfree--;
+        } else {
+            k++;
+        }
+    }
+}
+
+/* With the lock held: launch one wave from the oldest pending requests.
+ * Returns 1 when a wave was launched, 0 when nothing could be admitted. */
+static int admit(pose_b200_server_t *s)
+{
+    if (s->next_pending >= s->nreqs) return 0;
+    int w = -1;
+    for (uint32_t i = 0; i < s->max_waves; i++) if (!s->waves[i].busy) { w = (int)i; break; }
+    if (w < 0) return 0;
+    wave_t *wv = &s->waves[w];
+    size_t first = s->next_pending, last = s->nreqs; /* take everything pending */
+    size_t n = last - first;
+    pb_req_t *pr = (pb_req_t *)calloc(n, sizeof(*pr));
+    if (!pr) return 0;
+    for (size_t i = 0; i < n; i++) {
+        const sreq_t *r = &s->reqs[first + i];
+        pr[i].topo = r->topo;
+        pr[i].dev_ptr = r->dev_ptr;
+        pr[i].len = r->len;
+        pr[i].rbo = r->rbo;
+        pr[i].seed_off = s->sess_off[r->session];
+        pr[i].seed_len = s->sess_len[r->session];
+    }
+    pb_plan_tables_t pl;
+    uint32_t Tw = 4;
+    double eff = 0.0;
+    if (pb_plan_choose(pr, n, NULL, &Tw, &eff) != 0 || pb_plan_requests(pr, n, Tw, 32, eff, &pl) != 0) {
+        free(pr);
+        for (size_t i = first; i < last; i++) { s->reqs[i].state = 3; s->reqs[i].t_done = now_ms(); }
+        s->next_pending = last;
+        pthread_cond_broadcast(&s->cv);
+        return 1;
+    }
+    free(pr);
+    int launched = 0;
+    if (pl.nunits == 0) { /* nothing to label: done at once */
+        for (size_t i = first; i < last; i++) { s->reqs[i].state = 2; s->reqs[i].t_start = s->reqs[i].t_done = now_ms(); }
+        s->next_pending = last;
+        pthread_cond_broadcast(&s->cv);
+        pb_plan_free(&pl);
+        return 1;
+    }
+    /* teams: as many as fit in the largest free arena range, the GPU and the
+     * batches; CTAs of up to 256 threads, every team with its scratch */
+    const uint32_t tpc_max = 256 / (32 * Tw);
+    uint64_t cap = (uint64_t)pl.sms * (s->occ > 0 ? s->occ : 1) * tpc_max;
+    uint64_t R = arena_largest(s) / pl.team_scratch;
+    if (R > cap) R = cap;
+    if (R > pl.nbatches) R = pl.nbatches;
+    if (R == 0) { pb_plan_free(&pl); return 0; } /* wait for scratch to free up */
+    const uint32_t tpc = R < tpc_max ? (uint32_t)R : tpc_max;
+    const uint32_t g2 = (uint32_t)(R / tpc);
+    R = (uint64_t)g2 * tpc;
+    const uint64_t scratch = R * pl.team_scratch;
+    uint64_t off = 0;
+    if (arena_take(s, scratch, &off) != 0) { pb_plan_free(&pl); return 0; }
+    /* per-request completion counters (mapped host memory) */
+    if (wv->done_cap < n) {
+        if (wv->h_done) cudaFreeHost(wv->h_done);
+        wv->h_done = NULL;
+        wv->d_done = NULL;
+        wv->done_cap = 0;
+        size_t cap = n < 1024 ? 1024 : 2 * n;
+        if (cudaHostAlloc((void **)&wv->h_done, cap * sizeof(unsigned int), cudaHostAllocMapped) != cudaSuccess ||
+            cudaHostGetDevicePointer((void **)&wv->d_done, wv->h_done, 0) != cudaSuccess) {
+            if (wv->h_done) cudaFreeHost(wv->h_done);
+            wv->h_done = NULL;
+            cudaGetLastError();
+            arena_give(s, off, scratch);
+            pb_plan_free(&pl);
+            return 0;
+        }
+        wv->done_cap = cap;
+    }
+    if (wv->reqs_cap < n) {
+        uint64_t *nr = (uint64_t *)realloc(wv->reqs, n * sizeof(uint64_t));
+        if (nr) wv->reqs = nr;
+        uint32_t *nn = nr ? (uint32_t *)realloc(wv->need, n * sizeof(uint32_t)) : NULL;
+        if (nn) wv->need = nn;
+        if (!nr || !nn) { arena_give(s, off, scratch); pb_plan_free(&pl); return 0; }
+        wv->reqs_cap = n;
+    }
+    memset((void *)wv->h_done, 0, n * sizeof(unsigned int));
+    memset(wv->need, 0, n * sizeof(uint32_t));
+    for (uint64_t u = 0; u < pl.nunits; u++) wv->need[pl.unit_req[u]]++;
+    /* tables: views | batches | units | unit_req | jobs | seeds | queue, 256-byte aligned */
+    size_t o_views = 0, o_batches, o_units, o_ureq, o_jobs, o_seeds, o_queue, total;
+#define AL(x) (((x) + 255) & ~(size_t)255)
+    o_batches = AL(o_views + pl.ntopo * sizeof(pb_topo_view_t));
+    o_units = AL(o_batches + pl.nbatches * sizeof(pb_mbatch_t));
+    o_ureq = AL(o_units + pl.nunits * sizeof(pb_munit_t));
+    o_jobs = AL(o_ureq + pl.nunits * sizeof(uint32_t));
+    o_seeds = AL(o_jobs + pl.njobs * sizeof(pb_seedjob_t));
+    o_queue = AL(o_seeds + pl.njobs * 32);
+    total = AL(o_queue + 64);
+#undef AL
+    if (wv->tables_cap < total) {
+        cudaFree(wv->d_tables);
+        wv->d_tables = NULL;
+        wv->tables_cap = 0;
+        if (cudaMalloc(&wv->d_tables, total * 2) != cudaSuccess) { arena_give(s, off, scratch); pb_plan_free(&pl); return 0; }
+        wv->tables_cap = total * 2;
+    }
+    uint8_t *T = (uint8_t *)wv->d_tables;
+    int ok = 1;
+    ok &= cudaMemcpyAsync(T + o_views, pl.views, pl.ntopo * sizeof(pb_topo_view_t), cudaMemcpyHostToDevice, wv->stream) == cudaSuccess;
+    ok &= cudaMemcpyAsync(T + o_batches, pl.batches, pl.nbatches * sizeof(pb_mbatch_t), cudaMemcpyHostToDevice, wv->stream) == cudaSuccess;
+    ok &= cudaMemcpyAsync(T + o_units, pl.units, pl.nunits * sizeof(pb_munit_t), cudaMemcpyHostToDevice, wv->stream) == cudaSuccess;
+    ok &= cudaMemcpyAsync(T + o_ureq, pl.unit_req, pl.nunits * sizeof(uint32_t), cudaMemcpyHostToDevice, wv->stream) == cudaSuccess;
+    ok &= cudaMemcpyAsync(T + o_jobs, pl.jobs, pl.njobs * sizeof(pb_seedjob_t), cudaMemcpyHostToDevice, wv->stream) == cudaSuccess;
+    ok &= pb_dev_seed_jobs(T + o_jobs, (uint32_t)pl.njobs, s->d_sessions, (uint32_t *)(T + o_seeds), wv->stream) == 0;
+    ok &= cudaMemsetAsync(T + o_queue, 0, 64, wv->stream) == cudaSuccess;
+    pb_multi_params_t p;
+    memset(&p, 0, sizeof(p));
+    p.topos = (const pb_topo_view_t *)(T + o_views);
+    p.batches = (const pb_mbatch_t *)(T + o_batches);
+    p.units = (const pb_munit_t *)(T + o_units);
+    p.seeds = (const uint32_t *)(T + o_seeds);
+    p.scratch = s->d_arena + off;
+    p.team_scratch_bytes = pl.team_scratch;
+    p.nbatches = (uint32_t)pl.nbatches;
+    p.team_warps = Tw;
+    p.queue = (unsigned int *)(T + o_queue);
+    p.fma_adds = (double)R * Tw / pl.sms >= 8.0;
+    p.one = 1;
+    p.unit_req = (const uint32_t *)(T + o_ureq);
+    p.req_done = wv->d_done;
+    if (ok) ok = pb_dev_label_multi(&p, g2, 32 * Tw * tpc, wv->stream) == 0;
+    /* the range is zeroed before the wave counts as done */
+    if (ok) ok = cudaMemsetAsync(s->d_arena + off, 0, scratch, wv->stream) == cudaSuccess;
+    if (ok) ok = cudaEventRecord(wv->done, wv->stream) == cudaSuccess;
+    double t = now_ms();
+    if (!ok) {
+        fprintf(stderr, "pose_b200_server: wave launch failed: %s\n", cudaGetErrorString(cudaGetLastError()));
+        cudaStreamSynchronize(wv->stream);
+        arena_give(s, off, scratch);
+        for (size_t i = first; i < last; i++) { s->reqs[i].state = 3; s->reqs[i].t_done = t; }
+    } else {
+        wv->busy = 1;
+        wv->arena_off = off;
+        wv->arena_len = scratch;
+        wv->nreqs = n;
+        for (size_t i = 0; i < n; i++) {
+            wv->reqs[i] = first + i;
+            s->reqs[first + i].state = 1;
+            s->reqs[first + i].t_start = t;
+        }
+        s->waves_launched++;
+        launched = 1;
+    }
+    s->next_pending = last;
+    pb_plan_free(&pl);
+    pthread_cond_broadcast(&s->cv);
+    return launched || !ok;
+}
+
+/* With the lock held: complete the requests whose chunk copies are all in,
+ * and retire finished waves.  Returns how many requests or waves changed. */
+static int reap(pose_b200_server_t *s)
+{
+    int k = 0;
+    for (uint32_t i = 0; i < s->max_waves; i++) {
+        wave_t *wv = &s->waves[i];
+        if (!wv->busy) continue;
+        double t = now_ms();
+        for (size_t r = 0; r < wv->nreqs; r++) {
+            sreq_t *q = &s->reqs[wv->reqs[r]];
+            if (q->state == 1 && ((volatile unsigned int *)wv->h_done)[r] >= wv->need[r]) {
+                q->state = 2;
+                q->t_done = t;
+                k++;
+            }
+        }
+        cudaError_t e = cudaEventQuery(wv->done);
+        if (e == cudaErrorNotReady) continue;
+        t = now_ms();
+        for (size_t r = 0; r < wv->nreqs; r++) {
+            sreq_t *q = &s->reqs[wv->reqs[r]];
+            if (q->state == 1 || e != cudaSuccess) {
+                q->state = e == cudaSuccess ? 2 : 3;
+                q->t_done = t;
+            }
+        }
+        if (e != cudaSuccess) {
+            fprintf(stderr, "pose_b200_server: wave failed: %s\n", cudaGetErrorString(e));
+            cudaGetLastError();
+        }
+        arena_give(s, wv->arena_off, wv->arena_len);
+        wv->busy = 0;
+        k++;
+    }
+    if (k) pthread_cond_broadcast(&s->cv);
+    return k;
+}
+
+static void *dispatcher(void *arg)
+{
+    pose_b200_server_t *s = (pose_b200_server_t *)arg;
+    cudaSetDevice(s->device);
+    pthread_mutex_lock(&s->mu);
+    for (;;) {
+        int busy = 0;
+        for (uint32_t i = 0; i < s->max_waves; i++) busy |= s->waves[i].busy;
+        if (!s->running && !busy && s->next_pending >= s->nreqs) break;
+        int progress = reap(s);
+        while (admit(s)) progress = 1;
+        if (!progress) {
+            busy = 0;
+            for (uint32_t i = 0; i < s->max_waves; i++) busy |= s->waves[i].busy;
+            struct timespec ts;
+            clock_gettime(CLOCK_REALTIME, &ts);
+            long ns = busy ? 50000 : 2000000; /* poll running waves every 50 us */
+            ts.tv_nsec += ns;
+            if (ts.tv_nsec >= 1000000000L) { ts.tv_sec++; ts.tv_nsec -= 1000000000L; }
+            pthread_cond_timedwait(&s->cv, &s->mu, &ts);
+        }
+    }
+    pthread_mutex_unlock(&s->mu);
+    return NULL;
+}
+
+pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max_waves)
+{
+    pose_b200_server_t *s = (pose_b200_server_t *)calloc(1, sizeof(*s));
+    if (!s) return NULL;
+    cudaGetDevice(&s->device);
+    s->max_waves = max_waves ? (max_waves < PB_SERVER_MAX_WAVES ? max_waves : PB_SERVER_MAX_WAVES) : 4;
+    pthread_mutex_init(&s->mu, NULL);
+    pthread_cond_init(&s->cv, NULL);
+    if (scratch_bytes == 0) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        scratch_bytes = fr > ((uint64_t)8 << 30) ? (uint64_t)(fr / 2) : (uint64_t)(fr / 4);
+    }
+    scratch_bytes &= ~(uint64_t)255;
+    if (cudaMalloc((void **)&s->d_arena, scratch_bytes) != cudaSuccess) {
+        fprintf(stderr, "pose_b200_server_create: scratch arena of %llu bytes failed\n", (unsigned long long)scratch_bytes);
+        goto fail;
+    }
+    s->arena_bytes = scratch_bytes;
+    s->free_off[0] = 0;
+    s->free_len[0] = scratch_bytes;
+    s->nfree = 1;
+    for (uint32_t i = 0; i < s->max_waves; i++) {
+        if (cudaStreamCreateWithFlags(&s->waves[i].stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->waves[i].done, cudaEventDisableTiming) != cudaSuccess)
+            goto fail;
+    }
+    if (pb_dev_label_multi_occupancy(256, &s->occ) != 0) s->occ = 1;
+    s->running = 1;
+    if (pthread_create(&s->thread, NULL, dispatcher, s) != 0) { s->running = 0; goto fail; }
+    return s;
+fail:
+    cudaGetLastError();
+    for (uint32_t i = 0; i < s->max_waves; i++) {
+        if (s->waves[i].stream) cudaStreamDestroy(s->waves[i].stream);
+        if (s->waves[i].done) cudaEventDestroy(s->waves[i].done);
+    }
+    cudaFree(s->d_arena);
+    pthread_mutex_destroy(&s->mu);
+    pthread_cond_destroy(&s->cv);
+    free(s);
+    return NULL;
+}
+
+int pose_b200_server_session(pose_b200_server_t *s, const uint8_t *seed, size_t seed_len)
+{
+    if (!s || (!seed && seed_len) || seed_len > 1016) {
+        fprintf(stderr, "pose_b200_server_session: bad seed\n");
+        return -1;
+    }
+    pthread_mutex_lock(&s->mu);
+    int id = -1;
+    /* sessions are appended; the blob grows by copy (in-flight waves keep
+     * reading their own copy until they finish, so growth waits for idle) */
+    if (s->sess_bytes + seed_len > s->sess_cap) {
+        for (;;) {
+            int busy = 0;
+            for (uint32_t i = 0; i < s->max_waves; i++) busy |= s->waves[i].busy;
+            if (!busy && s->next_pending >= s->nreqs) break;
+            pthread_cond_wait(&s->cv, &s->mu);
+        }
+        size_t ncap = (s->sess_cap ? s->sess_cap * 2 : 4096);
+        while (ncap < s->sess_bytes + seed_len) ncap *= 2;
+        uint8_t *nb = NULL;
+        if (cudaMalloc((void **)&nb, ncap) != cudaSuccess) goto out;
+        if (s->sess_bytes && cudaMemcpy(nb, s->d_sessions, s->sess_bytes, cudaMemcpyDeviceToDevice) != cudaSuccess) {
+            cudaFree(nb);
+            goto out;
+        }
+        if (s->d_sessions) {
+            cudaMemset(s->d_sessions, 0, s->sess_cap);
+            cudaFree(s->d_sessions);
+        }
+        s->d_sessions = nb;
+        s->sess_cap = ncap;
+    }
+    if (s->nsess == s->sess_arr_cap) {
+        size_t nc = s->sess_arr_cap ? 2 * s->sess_arr_cap : 64;
+        uint32_t *a = (uint32_t *)realloc(s->sess_off, nc * 4), *b = a ? (uint32_t *)realloc(s->sess_len, nc * 4) : NULL;
+        if (!a || !b) { if (a) s->sess_off = a; goto out; }
+        s->sess_off = a;
+        s->sess_len = b;
+        s->sess_arr_cap = nc;
+    }
+    if (seed_len && cudaMemcpy(s->d_sessions + s->sess_bytes, seed, seed_len, cudaMemcpyHostToDevice) != cudaSuccess)
+        goto out;
+    s->sess_off[s->nsess] = (uint32_t)s->sess_bytes;
+    s->sess_len[s->nsess] = (uint32_t)seed_len;
+    s->sess_bytes += seed_len;
+    id = (int)s->nsess++;
+out:
+    pthread_mutex_unlock(&s->mu);
+    return id;
+}
+
+int64_t pose_b200_server_submit(pose_b200_server_t *s, const pose_hbm_topo_t *topo, int session, void *dev_ptr,
+                                size_t len, uint64_t region_block_offset)
+{
+    if (!s || !topo) return -1;
+    pthread_mutex_lock(&s->mu);
+    int64_t id = -1;
+    if (session < 0 || (size_t)session >= s->nsess) {
+        fprintf(stderr, "pose_b200_server_submit: unknown session %d\n", session);
+        goto out;
+    }
+    {
+        pb_topo_internal_t ti;
+        if (pb_topo_internal(topo, &ti) != 0 || ti.device != s->device) {
+            fprintf(stderr, "pose_b200_server_submit: topology of another device\n");
+            goto out;
+        }
+        if ((uint64_t)ti.view.pool * 32 > s->arena_bytes) {
+            fprintf(stderr, "pose_b200_server_submit: one chunk copy needs %llu bytes of scratch, the arena has %llu\n",
+                    (unsigned long long)ti.view.pool * 32, (unsigned long long)s->arena_bytes);
+            goto out;
+        }
+        if (len / ti.super_bytes && !dev_ptr) {
+            fprintf(stderr, "pose_b200_server_submit: NULL buffer\n");
+            goto out;
+        }
+    }
+    if (s->nreqs == s->reqs_cap) {
+        size_t nc = s->reqs_cap ? 2 * s->reqs_cap : 1024;
+        sreq_t *nr = (sreq_t *)realloc(s->reqs, nc * sizeof(sreq_t));
+        if (!nr) goto out;
+        s->reqs = nr;
+        s->reqs_cap = nc;
+    }
+    sreq_t *r = &s->reqs[s->nreqs];
+    memset(r, 0, sizeof(*r));
+    r->topo = topo;
+    r->dev_ptr = dev_ptr;
+    r->len = len;
+    r->rbo = region_block_offset;
+    r->session = session;
+    r->t_submit = now_ms();
+    id = (int64_t)s->nreqs++;
+    pthread_cond_broadcast(&s->cv);
+out:
+    pthread_mutex_unlock(&s->mu);
+    return id;
+}
+
+int pose_b200_server_wait(pose_b200_server_t *s, int64_t ticket, double *queue_ms, double *total_ms)
+{
+    if (!s || ticket < 0) return -1;
+    pthread_mutex_lock(&s->mu);
+    if ((size_t)ticket >= s->nreqs) { pthread_mutex_unlock(&s->mu); return -1; }
+    while (s->reqs[ticket].state < 2) pthread_cond_wait(&s->cv, &s->mu);
+    sreq_t r = s->reqs[ticket];
+    pthread_mutex_unlock(&s->mu);
+    if (queue_ms) *queue_ms = r.t_start - r.t_submit;
+    if (total_ms) *total_ms = r.t_done - r.t_submit;
+    return r.state == 2 ? 0 : -1;
+}
+
+int pose_b200_server_query(pose_b200_server_t *s, int64_t ticket)
+{
+    if (!s || ticket < 0) return -1;
+    pthread_mutex_lock(&s->mu);
+    int st = (size_t)ticket < s->nreqs ? s->reqs[ticket].state : 3;
+    pthread_mutex_unlock(&s->mu);
+    return st == 2 ? 1 : st == 3 ? -1 : 0;
+}
+
+void pose_b200_server_stats(pose_b200_server_t *s, uint64_t *submitted, uint64_t *waves, uint64_t *scratch_bytes)
+{
+    if (!s) return;
+    pthread_mutex_lock(&s->mu);
+    if (submitted) *submitted = s->nreqs;
+    if (waves) *waves = s->waves_launched;
+    if (scratch_bytes) *scratch_bytes = s->arena_bytes;
+    pthread_mutex_unlock(&s->mu);
+}
+
+void pose_b200_server_destroy(pose_b200_server_t *s)
+{
+    if (!s) return;
+    pthread_mutex_lock(&s->mu);
+    s->running = 0;
+    pthread_cond_broadcast(&s->cv);
+    pthread_mutex_unlock(&s->mu);
+    pthread_join(s->thread, NULL);
+    for (uint32_t i = 0; i < s->max_waves; i++) {
+        cudaStreamSynchronize(s->waves[i].stream);
+        cudaStreamDestroy(s->waves[i].stream);
+        cudaEventDestroy(s->waves[i].done);
+        cudaFree(s->waves[i].d_tables);
+        if (s->waves[i].h_done) cudaFreeHost(s->waves[i].h_done);
+        free(s->waves[i].reqs);
+        free(s->waves[i].need);
+    }
+    if (s->d_arena) {
+        cudaMemset(s->d_arena, 0, s->arena_bytes);
+        cudaFree(s->d_arena);
+    }
+    if (s->d_sessions) {
+        cudaMemset(s->d_sessions, 0, s->sess_cap);
+        cudaFree(s->d_sessions);
+    }
+    free(s->sess_off);
+    free(s->sess_len);
+    free(s->reqs);
+    pthread_mutex_destroy(&s->mu);
+    pthread_cond_destroy(&s->cv);
+    free(s);
+}

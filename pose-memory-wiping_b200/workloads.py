@@ -103,3 +103,17 @@ def copy_nodes(chunk_blocks: int) -> int:
 
 def chunk_nodes(chunk_blocks: int) -> int:
     return 2 * copy_nodes(chunk_blocks)
+
+
+def rank_region(workload: dict, rank: int, world: int) -> tuple[int, int]:
+    """(region_block_offset, super_chunks) of one rank under weak scaling:
+    every rank labels the workload's number of super-chunks, rank r taking
+    the r-th consecutive range of absolute positions.  No data crosses ranks:
+    a label depends only on (seed, absolute position), so the ranges are
+    independent and together equal one region of world * chunks super-chunks
+    (the K-GPUs-per-range split of tools/disk-wipe-bench/disk_wipe_bench.cu:
+    1016-1031, with each GPU given a whole range)."""
+    if not 0 <= rank < world:
+        raise ValueError("rank out of range")
+    cb, n = workload["chunk_blocks"], workload["chunks"]
+    return workload["rbo"] + rank * n * cb, n

@@ -68,9 +68,13 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-large", action="store_true", help="skip the 2^17 / 2^20 / batched digests")
     ap.add_argument("--threads", type=int, default=os.cpu_count() or 1)
+    ap.add_argument("--only-challenges", action="store_true", help="write challenges.json alone")
     args = ap.parse_args()
     ref = RefCPU()
     wl = _workloads()
+    if args.only_challenges:
+        challenges(ref, wl)
+        return
     rnd = random.Random(0xC0FFEE)
 
     # 1. official BLAKE3 vectors held by the reference test
@@ -171,7 +175,33 @@ def main() -> None:
                              "chunks": c4["chunks"], "rbo": c4["rbo"], "super_chunk_sha256": d,
                              "region_sha256": whole}
     json.dump(cfgs, open(cfg_path, "w"), indent=1)
+    challenges(ref, wl)
     print("golden fixtures written to", HERE)
+
+
+def challenges(ref, wl) -> None:
+    """6. verifier recompute: pose_graph_challenge on raw graph seeds, and
+    absolute region blocks of one session (chunk seed from the block's chunk
+    index) read out of the reference's region labeler."""
+    rnd = random.Random(0xC4A11)
+    graph = []
+    for m in [1, 2, 3, 5, 16, 17, 100, 1000, 1024, 4097, 1 << 12, 1 << 14]:
+        seed = bytes(rnd.randrange(256) for _ in range(32))
+        for idx in sorted({0, m - 1, rnd.randrange(m), rnd.randrange(m)}):
+            lab = ref.challenge(seed, m, idx)
+            assert lab is not None
+            graph.append({"seed": seed.hex(), "m": m, "index": idx, "hex": lab.hex()})
+        assert ref.challenge(seed, m, m) is None  # out of range
+    key = wl.splitmix64_key(7)
+    region = []
+    for cb in [64, 1000, 1024]:
+        chunks = sorted(rnd.sample(range(1 << 20), 5))
+        for J in chunks:
+            out = ref.label_super_chunks(key, cb, 1, J * cb, threads=1)
+            for r in sorted({0, cb - 1, rnd.randrange(cb)}):
+                region.append({"chunk_blocks": cb, "block": J * cb + r, "hex": out[32 * r:32 * r + 32].tobytes().hex()})
+    json.dump({"graph": graph, "region_key": key.hex(), "region": region},
+              open(os.path.join(HERE, "challenges.json"), "w"), indent=1)
 
 
 if __name__ == "__main__":

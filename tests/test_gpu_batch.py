@@ -1,0 +1,106 @@
+"""Batched labeling (one persistent launch over many sessions and chunk
+sizes, replayed from a captured CUDA graph) writes exactly the bytes each
+request gets from pose_graph_hbm_topo_label alone, and the 256-session
+workload's sampled chunks equal the reference CPU path's digests."""
+from __future__ import annotations
+
+import hashlib
+import random
+
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def test_batch_equals_individual_calls(pkg, cuda, oracle):
+    rnd = random.Random(3)
+    cbs = [1, 3, 16, 100, 1024, 4096]
+    topos = {cb: pkg.Topology(cb) for cb in cbs}
+    try:
+        reqs, bufs, want = [], [], []
+        for i in range(40):
+            cb = rnd.choice(cbs)
+            ns = rnd.randint(1, 6)
+            extra = rnd.choice([0, 0, 32 * rnd.randint(1, cb)]) if cb > 1 else 0
+            rbo = rnd.choice([0, cb * rnd.randrange(1 << 30), rnd.randrange(1 << 40)])
+            key = rnd.randbytes(rnd.choice([32, 32, 0, 9, 200]))
+            nbytes = ns * cb * 32 + extra
+            buf = cuda.full((nbytes,), 0x5C, dtype=cuda.uint8, device="cuda")
+            ref = cuda.full((nbytes,), 0x5C, dtype=cuda.uint8, device="cuda")
+            assert topos[cb].label(key, ref.data_ptr(), nbytes, rbo) == 0
+            reqs.append((topos[cb], key, buf.data_ptr(), nbytes, rbo))
+            bufs.append(buf)
+            want.append(ref)
+        with pkg.Batch(reqs) as b:
+            for _ in range(2):  # the captured graph replays identically
+                for t in bufs:
+                    t.fill_(0x5C)
+                rc, st = b.run()
+                assert rc == 0
+                cuda.cuda.synchronize()
+                for i, (t, r) in enumerate(zip(bufs, want)):
+                    assert cuda.equal(t, r), i
+        assert st["kernel"] == 4 and st["super_chunks"] == sum(r[3] // (r[0].chunk_blocks * 32) for r in reqs)
+        # spot-check against the CPU oracle
+        topo, key, _, nbytes, rbo = reqs[0]
+        ns = nbytes // (topo.chunk_blocks * 32)
+        assert bufs[0].cpu().numpy().tobytes()[: ns * topo.chunk_blocks * 32] == \
+            oracle.label_region(key, topo.chunk_blocks, ns, rbo, threads=4).tobytes()
+    finally:
+        for t in topos.values():
+            t.free()
+
+
+@pytest.mark.parametrize("sched", [None, {"team_warps": 2, "units_per_team": 4}, {"max_teams": 5}])
+def test_batch_schedules(pkg, cuda, oracle, sched):
+    topos = {cb: pkg.Topology(cb) for cb in (64, 512)}
+    try:
+        reqs, bufs = [], []
+        for i in range(12):
+            cb = 64 if i % 2 else 512
+            buf = cuda.zeros(3 * cb * 32, dtype=cuda.uint8, device="cuda")
+            reqs.append((topos[cb], bytes([i]) * 32, buf.data_ptr(), 3 * cb * 32, i * cb))
+            bufs.append(buf)
+        s = pkg.Sched(**sched) if sched else None
+        with pkg.Batch(reqs, s) as b:
+            rc, _ = b.run()
+            assert rc == 0
+        for (topo, key, _, nbytes, rbo), buf in zip(reqs, bufs):
+            want = oracle.label_region(key, topo.chunk_blocks, 3, rbo, threads=4).tobytes()
+            assert buf.cpu().numpy().tobytes() == want
+    finally:
+        for t in topos.values():
+            t.free()
+
+
+def test_batched_256_sessions_sampled_vs_reference(pkg, cuda, wl):
+    rows = {r["session"]: r for r in golden("configs.json")["batched_sampled"]}
+    sessions = wl.batched()
+    cbs = sorted({s["chunk_blocks"] for s in sessions})
+    topos = {cb: pkg.Topology(cb) for cb in cbs}
+    try:
+        total = sum(s["chunk_blocks"] * 32 * len(s["chunk_indices"]) for s in sessions)
+        big = cuda.zeros(total, dtype=cuda.uint8, device="cuda")
+        reqs, first_off = [], {}
+        off = 0
+        for s in sessions:
+            cb = s["chunk_blocks"]
+            for k, idx in enumerate(s["chunk_indices"]):
+                if k == 0:
+                    first_off[s["session"]] = off
+                reqs.append((topos[cb], s["key"], big.data_ptr() + off, cb * 32, idx * cb))
+                off += cb * 32
+        with pkg.Batch(reqs) as b:
+            rc, st = b.run()
+        assert rc == 0
+        host = big.cpu().numpy()
+        for s in sessions:
+            r = rows[s["session"]]
+            o = first_off[s["session"]]
+            got = hashlib.sha256(host[o:o + r["chunk_blocks"] * 32].tobytes()).hexdigest()
+            assert got == r["sha256"], s["session"]
+    finally:
+        for t in topos.values():
+            t.free()

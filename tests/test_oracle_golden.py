@@ -103,3 +103,23 @@ def test_scaffold_labels_match_reference_order(oracle):
     for m in [1, 2, 5, 16, 64]:
         _, allb = oracle.label_chunk(cs, m, with_all=True)
         assert (allb == ref.scaffold_labels(cs, m)).all()
+
+
+def test_challenges(oracle):
+    """Verifier recompute: the oracle's chunk labeler answers the reference's
+    pose_graph_challenge (graph.c:1019-1042) on raw graph seeds, and region
+    blocks of one session (chunk seed from the block's chunk index)."""
+    ch = golden("challenges.json")
+    memo = {}
+    for c in ch["graph"]:
+        key = (c["seed"], c["m"])
+        if key not in memo:
+            memo[key] = oracle.label_chunk(bytes.fromhex(c["seed"]), c["m"])
+        r = c["index"]
+        assert memo[key][32 * r:32 * r + 32].tobytes().hex() == c["hex"], (c["m"], r)
+    skey = bytes.fromhex(ch["region_key"])
+    for c in ch["region"]:
+        cb, b = c["chunk_blocks"], c["block"]
+        out = oracle.label_region(skey, cb, 1, (b // cb) * cb)
+        r = b % cb
+        assert out[32 * r:32 * r + 32].tobytes().hex() == c["hex"], (cb, b)
