@@ -2,7 +2,8 @@
 """Benchmark of the PoSE-DB labeling hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload plain_2e17|plain_small|window_2e17]
+                    [--workload plain_2e17|plain_small|window_2e17|throughput_2e12|
+                                latency_2e14|batched|served] [--no-aux] [--no-cpu-baseline]
 
 One step = one pass of the hot path over one batch: label the workload's
 super-chunks (default: 32 consecutive super-chunks at chunk_blocks = 2^17,
@@ -11,6 +12,11 @@ pose_graph_hbm_topo_label with the topology resident, as disk-wipe-bench's
 worker does per HBM window.  Metric: persisted label MiB/s
 (chunk_blocks*32 bytes per super-chunk / time), the reference's own
 definition (common/src/cuda/label_gpu_common.cu:312-315).
+
+At one GPU the default run adds, under their own keys: a full 16 GiB window
+at 2^17 (the throughput regime), the 256-session batched workload in one
+autotuned persistent launch, and a 120-request Poisson trace through the
+continuous-batching server next to the same trace run one request at a time.
 
 Under torchrun each rank labels its own disjoint range of super-chunks
 (absolute positions offset by rank): no collective on the data path, weak
@@ -171,6 +177,35 @@ def run_reference_arm(args) -> None:
 
 # ── B200 arm ────────────────────────────────────────────────────────────────
 
+def run_window(pkg, torch, topo, rate: float, reps: int = 1) -> dict:
+    """A full reference-sized HBM window at chunk_blocks 2^17: 4096
+    super-chunks (16 GiB, the default window of disk-wipe-bench), key
+    splitmix64(1), from absolute position 0 — the throughput regime, where the
+    INT32 roofline binds."""
+    w = workload("window_2e17")
+    nbytes = w["chunks"] * w["chunk_blocks"] * 32
+    buf = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    rc = topo.label(w["key"], buf.data_ptr(), nbytes, 0)  # warm-up
+    assert rc == 0, pkg.last_error()
+    best = None
+    for _ in range(reps):
+        rc, st = topo.label(w["key"], buf.data_ptr(), nbytes, 0, stats=True)
+        assert rc == 0, pkg.last_error()
+        if best is None or st["total_ms"] < best["total_ms"]:
+            best = st
+    del buf
+    comps = 2 if best["used_cv0_table"] else 3
+    achieved = best["nodes"] * comps * 680.0 / (best["kernel_ms"] * 1e-3)
+    peak = rate * 680.0
+    return {"workload": "window_2e17: 4096 super-chunks of chunk_blocks 2^17 (16 GiB), key splitmix64(1)",
+            "value": nbytes / MIB / (best["total_ms"] * 1e-3), "unit": "MiB/s", "ms": best["total_ms"],
+            "kernel_ms": best["kernel_ms"], "kernel": best["kernel"],
+            "schedule": {"T": best["team_warps"], "G": best["units_per_team"], "teams": best["teams"]},
+            "roofline": {"bound": "int32", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s",
+                         "frac": achieved / peak,
+                         "frac_of_spec_method": best["nodes"] * 3 * 680.0 / (best["kernel_ms"] * 1e-3) / peak}}
+
+
 def run_batched(pkg, torch, sched=None, reps: int = 2) -> dict:
     """The batched workload (256 sessions, chunk_blocks 2^12..2^17, 1-8 chunks
     each at random absolute positions) through one persistent launch replayed
@@ -187,7 +222,8 @@ def run_batched(pkg, torch, sched=None, reps: int = 2) -> dict:
             reqs.append((topos[cb], s["key"], big.data_ptr() + off, cb * 32, idx * cb))
             off += cb * 32
     best = None
-    with pkg.Batch(reqs, sched) as b:
+    with pkg.Batch(reqs, sched, autotune=0 if sched is not None else 3) as b:
+        chosen = b.chosen
         b.run()  # warm-up replay
         for _ in range(reps):
             rc, st = b.run()
@@ -200,7 +236,10 @@ def run_batched(pkg, torch, sched=None, reps: int = 2) -> dict:
             "value": total / MIB / (best["total_ms"] * 1e-3), "unit": "MiB/s",
             "graph_ms": best["total_ms"], "super_chunks": best["super_chunks"], "units": best["units"],
             "nodes": best["nodes"], "teams": best["teams"], "team_warps": best["team_warps"],
-            "max_units_per_team": best["units_per_team"], "kernel_launches_per_replay": 2}
+            "max_units_per_team": best["units_per_team"], "kernel_launches_per_replay": 2,
+            "schedule": "autotuned" if chosen else "given",
+            "packing": None if not chosen else ("chain-bounded" if chosen["lane_efficiency"] == pkg.PACK_CHAIN
+                                                 else f"lane efficiency {chosen['lane_efficiency']}%")}
 
 
 def run_served(pkg, torch, requests: int = 300, alone: bool = False) -> dict:
@@ -288,6 +327,8 @@ def run_b200(args) -> None:
                                 device_id=torch.device("cuda", local))
     os.environ.setdefault("POSE_GPU_QUIET", "1")
     w = workload(args.workload)
+    if args.chunks:
+        w = dict(w, chunks=args.chunks, name=f"{w['name']} ({args.chunks} super-chunks)")
     cb, nsup = w["chunk_blocks"], w["chunks"]
     sb = cb * 32
     nbytes = nsup * sb
@@ -379,6 +420,7 @@ def run_b200(args) -> None:
         "kernel_ms": kernel_ms,
     }
     if world == 1 and not args.no_aux and args.workload == "plain_2e17":
+        line["window_2e17"] = run_window(pkg, torch, topo, rate)
         line["batched"] = run_batched(pkg, torch)
         line["served"] = run_served(pkg, torch, requests=120, alone=True)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -417,6 +459,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="plain_2e17")
+    ap.add_argument("--chunks", type=int, default=0, help="override the workload's super-chunk count (profiling)")
     ap.add_argument("--no-cv0", action="store_true", help="hash block 0 in every call (no table)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-aux", action="store_true", help="skip the batched and served legs")

@@ -27,9 +27,12 @@ typedef struct {
                                    3 = warp-specialised kernel (team_warps = hashing warps: 7 or 15) */
     uint64_t scratch_cap_bytes; /* cap on the scratch pool (0 = free HBM less a margin) */
     uint32_t lane_efficiency;   /* batched launches: per-topology G reaches this lane efficiency,
-                                   in percent (0 = automatic) */
+                                   in percent; POSE_B200_PACK_CHAIN packs units while their chain
+                                   stays within the launch's longest; 0 = automatic */
     uint32_t reserved;
 } pose_b200_sched_t;
+
+#define POSE_B200_PACK_CHAIN 255u
 
 /* What one call did (device times from CUDA events on the labeler's stream). */
 typedef struct {
@@ -101,6 +104,15 @@ typedef struct pose_b200_batch pose_b200_batch_t;
  * by the makespan estimate. */
 pose_b200_batch_t *pose_b200_batch_create(const pose_b200_request_t *reqs, size_t n,
                                           const pose_b200_sched_t *sched);
+/* The empirical autotuner: rank the schedules sched leaves open (team size
+ * 1/2/4/8 and the packing rule) by the makespan estimate, capture the best
+ * `trials` of them (0 = 3), time one replay of each, and return the fastest
+ * batch, already captured; *chosen (may be NULL) gets its schedule, which
+ * pose_b200_batch_create reproduces, and *stats its timed replay.  Every
+ * replay writes the same bytes.  NULL on error. */
+pose_b200_batch_t *pose_b200_batch_autotune(const pose_b200_request_t *reqs, size_t n,
+                                            const pose_b200_sched_t *sched, uint32_t trials,
+                                            pose_b200_sched_t *chosen, pose_b200_stats_t *stats);
 /* Replay the captured launch (synchronous).  0 on success, -1 on error. */
 int pose_b200_batch_run(pose_b200_batch_t *batch, pose_b200_stats_t *stats);
 /* Zero the batch's scratch and seeds, free it. */

@@ -41,6 +41,9 @@ class Sched(C.Structure):
                 ("reserved", C.c_uint32)]
 
 
+PACK_CHAIN = 255  # POSE_B200_PACK_CHAIN: pack units while their chain stays within the launch's longest
+
+
 class Stats(C.Structure):
     """pose_b200_stats_t."""
 
@@ -108,6 +111,9 @@ def _declare(L: C.CDLL) -> None:
     L.pose_b200_topo_label_noalloc.restype = C.c_int
     L.pose_b200_batch_create.argtypes = [C.POINTER(Request), C.c_size_t, C.POINTER(Sched)]
     L.pose_b200_batch_create.restype = C.c_void_p
+    L.pose_b200_batch_autotune.argtypes = [C.POINTER(Request), C.c_size_t, C.POINTER(Sched), C.c_uint32,
+                                           C.POINTER(Sched), C.POINTER(Stats)]
+    L.pose_b200_batch_autotune.restype = C.c_void_p
     L.pose_b200_batch_run.argtypes = [C.c_void_p, C.POINTER(Stats)]
     L.pose_b200_batch_run.restype = C.c_int
     L.pose_b200_batch_destroy.argtypes = [C.c_void_p]
@@ -307,16 +313,29 @@ class Batch:
     """pose_b200_batch_t: many requests in one persistent launch, captured once
     into a CUDA graph and replayed by run().
 
-    requests: iterable of (topology, seed bytes, device pointer, nbytes, rbo)."""
+    requests: iterable of (topology, seed bytes, device pointer, nbytes, rbo).
+    autotune > 0 runs pose_b200_batch_autotune with that many trials; the
+    chosen schedule is then in .chosen and its timed replay in .tune_stats."""
 
-    def __init__(self, requests, sched: Sched | None = None):
+    def __init__(self, requests, sched: Sched | None = None, autotune: int = 0):
         reqs = list(requests)
         self._seeds = [C.create_string_buffer(bytes(r[1]), max(1, len(r[1]))) for r in reqs]
         arr = (Request * len(reqs))()
         for i, (topo, seed, ptr, nbytes, rbo) in enumerate(reqs):
             arr[i] = Request(topo.handle, C.cast(self._seeds[i], C.c_void_p), len(seed), ptr, nbytes, rbo)
         self._arr = arr
-        h = load().pose_b200_batch_create(arr, len(reqs), C.byref(sched) if sched is not None else None)
+        self.chosen = None
+        self.tune_stats = None
+        sp = C.byref(sched) if sched is not None else None
+        if autotune:
+            ch = Sched()
+            st = Stats()
+            h = load().pose_b200_batch_autotune(arr, len(reqs), sp, autotune, C.byref(ch), C.byref(st))
+            if h:
+                self.chosen = {k: getattr(ch, k) for k, _ in ch._fields_}
+                self.tune_stats = st.as_dict()
+        else:
+            h = load().pose_b200_batch_create(arr, len(reqs), sp)
         if not h:
             raise RuntimeError("batch create failed")
         self.handle = h

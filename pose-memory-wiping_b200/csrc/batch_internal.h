@@ -47,6 +47,16 @@ int pb_plan_requests(const pb_req_t *reqs, size_t n, uint32_t T, uint32_t gcap, 
  * all nodes spread over the SMs. */
 double pb_plan_makespan(const pb_plan_tables_t *p, uint32_t T, uint64_t R);
 void pb_plan_free(pb_plan_tables_t *p);
+/* A schedule candidate: team size, packing rule (eff_min of
+ * pb_plan_requests) and its estimated makespan. */
+typedef struct {
+    uint32_t T;
+    double eff;
+    double est;
+} pb_cand_t;
+/* The candidates sched leaves open (T in 1, 2, 4, 8; four packing rules),
+ * best estimate first; returns their number (at most cap) or -1. */
+int pb_plan_rank(const pb_req_t *reqs, size_t n, const pose_b200_sched_t *sched, pb_cand_t *out, int cap);
 /* Team size T (1, 2, 4 or 8, unless sched fixes it) and packing rule for
  * pb_plan_requests with the lowest estimated makespan. */
 int pb_plan_choose(const pb_req_t *reqs, size_t n, const pose_b200_sched_t *sched, uint32_t *T, double *eff_min);

@@ -245,29 +245,48 @@ double pb_plan_makespan(const pb_plan_tables_t *p, uint32_t T, uint64_t R)
     return (chain > alu ? chain : alu) * waves;
 }
 
-int pb_plan_choose(const pb_req_t *pr, size_t n, const pose_b200_sched_t *sched, uint32_t *T_out, double *eff_out)
+static int cmp_cand(const void *a, const void *b)
 {
-    /* the lowest estimated makespan over the team sizes and packing rules
-     * (chain-bounded, or a lane-efficiency target) the caller left open */
+    double x = ((const pb_cand_t *)a)->est, y = ((const pb_cand_t *)b)->est;
+    return x < y ? -1 : x > y;
+}
+
+int pb_plan_rank(const pb_req_t *pr, size_t n, const pose_b200_sched_t *sched, pb_cand_t *out, int cap)
+{
+    /* every team size and packing rule the caller left open, by estimated
+     * makespan (chain-bounded packing, or a lane-efficiency target) */
     const uint32_t gcap = sched && sched->units_per_team ? sched->units_per_team : 32;
     const uint32_t t_lo = sched && sched->team_warps ? sched->team_warps : 1;
     const uint32_t t_hi = sched && sched->team_warps ? sched->team_warps : 8;
     double rules[4] = {0.0, 0.5, 0.7, 0.85};
     int nrules = 4;
     if (sched && sched->lane_efficiency) {
-        rules[0] = sched->lane_efficiency / 100.0;
+        rules[0] = sched->lane_efficiency == POSE_B200_PACK_CHAIN ? 0.0 : sched->lane_efficiency / 100.0;
         nrules = 1;
     }
-    double best = -1;
+    int k = 0;
     for (uint32_t tT = t_lo; tT <= t_hi; tT <<= 1) {
-        for (int e = 0; e < nrules; e++) {
+        for (int e = 0; e < nrules && k < cap; e++) {
             pb_plan_tables_t cand;
             if (pb_plan_requests(pr, n, tT, gcap, rules[e], &cand) != 0) return -1;
-            double ms = pb_plan_makespan(&cand, tT, (uint64_t)cand.sms * 32 / tT);
-            if (best < 0 || ms < best) { best = ms; *T_out = tT; *eff_out = rules[e]; }
+            out[k].T = tT;
+            out[k].eff = rules[e];
+            out[k].est = pb_plan_makespan(&cand, tT, (uint64_t)cand.sms * 32 / tT);
+            k++;
             pb_plan_free(&cand);
         }
     }
+    qsort(out, (size_t)k, sizeof(*out), cmp_cand);
+    return k;
+}
+
+int pb_plan_choose(const pb_req_t *pr, size_t n, const pose_b200_sched_t *sched, uint32_t *T_out, double *eff_out)
+{
+    pb_cand_t c[16];
+    int k = pb_plan_rank(pr, n, sched, c, 16);
+    if (k <= 0) return -1;
+    *T_out = c[0].T;
+    *eff_out = c[0].eff;
     return 0;
 }
 
@@ -286,6 +305,10 @@ pose_b200_batch_t *pose_b200_batch_create(const pose_b200_request_t *reqs, size_
     if (sched && sched->team_warps && sched->team_warps != 1 && sched->team_warps != 2 && sched->team_warps != 4 &&
         sched->team_warps != 8) {
         fprintf(stderr, "pose_b200_batch_create: team_warps must be 1, 2, 4 or 8\n");
+        return NULL;
+    }
+    if (sched && sched->lane_efficiency > 100 && sched->lane_efficiency != POSE_B200_PACK_CHAIN) {
+        fprintf(stderr, "pose_b200_batch_create: lane_efficiency must be a percentage or POSE_B200_PACK_CHAIN\n");
         return NULL;
     }
     for (size_t i = 0; i < n; i++) {
@@ -454,4 +477,52 @@ int pose_b200_label_batch(const pose_b200_request_t *reqs, size_t n, const pose_
     int rc = pose_b200_batch_run(b, stats);
     pose_b200_batch_destroy(b);
     return rc;
+}
+
+pose_b200_batch_t *pose_b200_batch_autotune(const pose_b200_request_t *reqs, size_t n, const pose_b200_sched_t *sched,
+                                            uint32_t trials, pose_b200_sched_t *chosen, pose_b200_stats_t *stats)
+{
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (!reqs || n == 0) { fprintf(stderr, "pose_b200_batch_autotune: no requests\n"); return NULL; }
+    pb_req_t *pr = (pb_req_t *)calloc(n, sizeof(*pr));
+    if (!pr) return NULL;
+    for (size_t i = 0; i < n; i++) { /* the ranking needs no seeds */
+        pr[i].topo = reqs[i].topo;
+        pr[i].dev_ptr = reqs[i].hbm_dev_ptr;
+        pr[i].len = reqs[i].hbm_len;
+        pr[i].rbo = reqs[i].region_block_offset;
+    }
+    pb_cand_t c[16];
+    int k = pb_plan_rank(pr, n, sched, c, 16);
+    free(pr);
+    if (k <= 0) return NULL;
+    if (trials == 0) trials = 3;
+    if ((int)trials < k) k = (int)trials;
+    pose_b200_batch_t *best = NULL;
+    double best_ms = 0;
+    for (int i = 0; i < k; i++) {
+        pose_b200_sched_t s;
+        if (sched) s = *sched;
+        else memset(&s, 0, sizeof(s));
+        s.team_warps = c[i].T;
+        s.lane_efficiency = c[i].eff > 0 ? (uint32_t)(c[i].eff * 100.0 + 0.5) : POSE_B200_PACK_CHAIN;
+        pose_b200_batch_t *b = pose_b200_batch_create(reqs, n, &s);
+        if (!b) continue;
+        pose_b200_stats_t st;
+        /* the first replay of a process pays one-time costs: warm up once */
+        int rc = best ? 0 : pose_b200_batch_run(b, NULL);
+        if (rc == 0) rc = pose_b200_batch_run(b, &st);
+        if (rc != 0) { pose_b200_batch_destroy(b); continue; }
+        if (!best || st.total_ms < best_ms) {
+            pose_b200_batch_destroy(best);
+            best = b;
+            best_ms = st.total_ms;
+            if (chosen) *chosen = s;
+            if (stats) *stats = st;
+        } else {
+            pose_b200_batch_destroy(b);
+        }
+    }
+    if (!best) fprintf(stderr, "pose_b200_batch_autotune: no candidate schedule ran\n");
+    return best;
 }

@@ -518,11 +518,22 @@ extern "C" int pb_dev_chunk_seeds(const uint8_t *d_session_seed, uint32_t seed_l
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
+/* k_label's 512-thread CTAs stage 48 KiB, which with the static shared
+ * memory is above the default per-CTA limit: opt in (idempotent). */
+static void allow_stage_smem()
+{
+    const int bytes = (int)(PB_PREF_BYTES_PER_THREAD * PB_CTA_THREADS);
+    cudaFuncSetAttribute(pb::k_label<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(pb::k_label<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
 extern "C" int pb_dev_label(const pb_label_params_t *params, uint32_t grid, uint32_t cta_threads,
                             cudaStream_t stream)
 {
     cudaGetLastError(); /* report only this launch */
     const uint32_t smem = PB_PREF_BYTES_PER_THREAD * cta_threads;
+    if (smem > 48 * 1024 - 1024) allow_stage_smem();
+    cudaGetLastError();
     if (params->fma_adds) pb::k_label<true><<<grid, cta_threads, smem, stream>>>(*params);
     else pb::k_label<false><<<grid, cta_threads, smem, stream>>>(*params);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
@@ -563,6 +574,7 @@ extern "C" int pb_dev_label_occupancy(uint32_t cta_threads, int *blocks_per_sm)
 {
     int a = 0, b = 0;
     const size_t smem = PB_PREF_BYTES_PER_THREAD * cta_threads;
+    allow_stage_smem();
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, pb::k_label<false>, (int)cta_threads, smem) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, pb::k_label<true>, (int)cta_threads, smem) != cudaSuccess)
         return -1;

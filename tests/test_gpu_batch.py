@@ -53,7 +53,9 @@ def test_batch_equals_individual_calls(pkg, cuda, oracle):
             t.free()
 
 
-@pytest.mark.parametrize("sched", [None, {"team_warps": 2, "units_per_team": 4}, {"max_teams": 5}])
+@pytest.mark.parametrize("sched", [None, {"team_warps": 2, "units_per_team": 4}, {"max_teams": 5},
+                                   {"team_warps": 8, "lane_efficiency": 255}, {"team_warps": 1, "lane_efficiency": 70},
+                                   {"team_warps": 4, "units_per_team": 1}, "autotune"])
 def test_batch_schedules(pkg, cuda, oracle, sched):
     topos = {cb: pkg.Topology(cb) for cb in (64, 512)}
     try:
@@ -63,8 +65,13 @@ def test_batch_schedules(pkg, cuda, oracle, sched):
             buf = cuda.zeros(3 * cb * 32, dtype=cuda.uint8, device="cuda")
             reqs.append((topos[cb], bytes([i]) * 32, buf.data_ptr(), 3 * cb * 32, i * cb))
             bufs.append(buf)
-        s = pkg.Sched(**sched) if sched else None
-        with pkg.Batch(reqs, s) as b:
+        s = pkg.Sched(**sched) if isinstance(sched, dict) else None
+        with pkg.Batch(reqs, s, autotune=3 if sched == "autotune" else 0) as b:
+            if sched == "autotune":
+                assert b.chosen["team_warps"] in (1, 2, 4, 8)
+                assert b.chosen["lane_efficiency"] in (50, 70, 85, pkg.PACK_CHAIN)
+                for t in bufs:
+                    t.zero_()
             rc, _ = b.run()
             assert rc == 0
         for (topo, key, _, nbytes, rbo), buf in zip(reqs, bufs):
@@ -104,3 +111,11 @@ def test_batched_256_sessions_sampled_vs_reference(pkg, cuda, wl):
     finally:
         for t in topos.values():
             t.free()
+
+
+def test_batch_rejects_bad_schedules(pkg, cuda):
+    with pkg.Topology(64) as t:
+        buf = cuda.zeros(64 * 32, dtype=cuda.uint8, device="cuda")
+        for bad in ({"team_warps": 3}, {"team_warps": 16}, {"lane_efficiency": 101}):
+            with pytest.raises(RuntimeError):
+                pkg.Batch([(t, b"k" * 32, buf.data_ptr(), 64 * 32, 0)], pkg.Sched(**bad))
