@@ -70,6 +70,20 @@ void pose_b200_topo_info(const pose_hbm_topo_t *topo, uint32_t *chunk_blocks,
 int pose_b200_plan(const pose_hbm_topo_t *topo, uint64_t super_chunks,
                    const pose_b200_sched_t *hint, pose_b200_sched_t *out);
 
+/* Timed-trial autotuner for one call shape.  It has no counterpart in the
+ * reference; it tunes pose_graph_hbm_topo_label (common/include/gpu_label.h:
+ * 80-83).  It ranks the modelled best schedule of every team size of the
+ * basic kernel and the depth kernel, runs the `trials` cheapest of them
+ * (0 = 4) as real labeling calls on the given buffer, and remembers the
+ * fastest: later calls on this topology with the same number of super-chunks
+ * and no explicit schedule use it.  The buffer ends up holding the labels,
+ * exactly as after pose_graph_hbm_topo_label.  Returns 0, or -1 on error;
+ * `chosen` (may be NULL) gets the winning schedule and `stats` (may be NULL)
+ * its timed call.  Same threading rule as the labeling call. */
+int pose_b200_topo_autotune(pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
+                            void *hbm_dev_ptr, size_t hbm_len, uint64_t region_block_offset,
+                            uint32_t trials, pose_b200_sched_t *chosen, pose_b200_stats_t *stats);
+
 /* Sustained compression rate of this GPU for the labeler's instruction mix:
  * every SM full of threads chaining register-resident compressions.  Returns
  * compressions per second (0 on error); *latency_cycles gets the dependent

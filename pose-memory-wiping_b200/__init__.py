@@ -104,6 +104,9 @@ def _declare(L: C.CDLL) -> None:
     L.pose_b200_topo_info.restype = None
     L.pose_b200_plan.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(Sched), C.POINTER(Sched)]
     L.pose_b200_plan.restype = C.c_int
+    L.pose_b200_topo_autotune.argtypes = [C.c_void_p, _u8p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_uint64,
+                                          C.c_uint32, C.POINTER(Sched), C.POINTER(Stats)]
+    L.pose_b200_topo_autotune.restype = C.c_int
     L.pose_b200_compress_rate.argtypes = [C.c_uint32, C.POINTER(C.c_double)]
     L.pose_b200_compress_rate.restype = C.c_double
     L.pose_b200_topo_label_noalloc.argtypes = [C.c_void_p, _u8p, C.c_size_t, C.c_void_p, C.c_size_t,
@@ -213,6 +216,18 @@ class Topology:
                                     nbytes, region_block_offset,
                                     C.byref(sched) if sched is not None else None, C.byref(st))
         return (rc, st.as_dict()) if stats else rc
+
+    def autotune(self, seed: bytes, dev_ptr: int, nbytes: int, region_block_offset: int = 0,
+                 trials: int = 4):
+        """pose_b200_topo_autotune: time the best modelled schedule of each
+        team size on this call and keep the fastest for later calls of the
+        same size.  Returns (rc, chosen schedule dict, stats dict); the
+        buffer holds the labels afterwards."""
+        ch = Sched()
+        st = Stats()
+        rc = load().pose_b200_topo_autotune(self.handle, _bytes_arg(seed), len(seed), C.c_void_p(dev_ptr), nbytes,
+                                            region_block_offset, trials, C.byref(ch), C.byref(st))
+        return rc, {k: getattr(ch, k) for k, _ in Sched._fields_}, st.as_dict()
 
     def label_noalloc(self, seed: bytes, dev_ptr: int, nbytes: int, region_block_offset: int = 0) -> int:
         """pose_b200_topo_label_noalloc: the same bytes as label(), with the

@@ -91,6 +91,10 @@ struct pose_hbm_topo {
     size_t sess_alloc;
     unsigned int *d_queue;
     int occ256, occ512, sms;
+    /* schedule chosen by pose_b200_topo_autotune for calls of tuned_units chunk copies */
+    int tuned_ok;
+    uint64_t tuned_units;
+    pose_b200_sched_t tuned;
 };
 
 /* ── schedule model ──────────────────────────────────────────────────────── */
@@ -519,6 +523,73 @@ int pose_b200_plan(const pose_hbm_topo_t *t, uint64_t super_chunks, const pose_b
     return 0;
 }
 
+static int topo_label_core(const pose_hbm_topo_t *ct, const uint8_t *session_seed, size_t seed_len,
+                           const uint8_t *raw_seeds, void *hbm_dev_ptr, size_t hbm_len, uint64_t rbo,
+                           const pose_b200_sched_t *sched, pose_b200_stats_t *stats);
+
+/* Candidates of the autotuner: the modelled best schedule of every team size
+ * of the basic kernel and the depth kernel, cheapest model cost first. */
+static int autotune_candidates(pose_hbm_topo_t *t, uint64_t nunits, uint64_t budget, pose_b200_sched_t *c,
+                               double *cost, int max)
+{
+    int n = 0;
+    for (uint32_t k = 0; k < 6 && n < max; k++) {
+        pose_b200_sched_t h;
+        memset(&h, 0, sizeof(h));
+        if (k < 5) { h.kernel = 1; h.team_warps = 1u << k; }
+        else h.kernel = 3;
+        plan_t p;
+        if (make_plan(t, nunits, &h, budget, &p) != 0) continue;
+        pose_b200_sched_t s;
+        memset(&s, 0, sizeof(s));
+        s.kernel = p.kernel;
+        s.team_warps = p.T;
+        s.units_per_team = p.G;
+        s.max_teams = p.teams;
+        int i = n++;
+        while (i > 0 && cost[i - 1] > p.cost) { c[i] = c[i - 1]; cost[i] = cost[i - 1]; i--; }
+        c[i] = s;
+        cost[i] = p.cost;
+    }
+    return n;
+}
+
+int pose_b200_topo_autotune(pose_hbm_topo_t *t, const uint8_t *session_seed, size_t seed_len, void *hbm_dev_ptr,
+                            size_t hbm_len, uint64_t region_block_offset, uint32_t trials,
+                            pose_b200_sched_t *chosen, pose_b200_stats_t *stats)
+{
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (!t) { set_err("pose_b200_topo_autotune: NULL topology"); return -1; }
+    const uint64_t num_super = hbm_len / t->super_bytes;
+    if (num_super == 0) { set_err("pose_b200_topo_autotune: buffer smaller than one super-chunk"); return -1; }
+    const uint64_t per_launch = num_super < PB_MAX_CHUNKS_PER_LAUNCH ? num_super : PB_MAX_CHUNKS_PER_LAUNCH;
+    const uint64_t nunits = per_launch * t->copies;
+    pose_b200_sched_t c[6];
+    double cost[6];
+    t->tuned_ok = 0;
+    const int n = autotune_candidates(t, nunits, scratch_budget(t, NULL), c, cost, 6);
+    if (n <= 0) { set_err("pose_b200_topo_autotune: no schedule fits the scratch budget"); return -1; }
+    const int k = (int)(trials == 0 ? 4u : trials) < n ? (int)(trials == 0 ? 4u : trials) : n;
+    int best = -1;
+    pose_b200_stats_t bst;
+    memset(&bst, 0, sizeof(bst));
+    for (int i = 0; i < k; i++) {
+        pose_b200_stats_t st;
+        if (topo_label_core(t, session_seed, seed_len, NULL, hbm_dev_ptr, hbm_len, region_block_offset, &c[i],
+                            &st) != 0)
+            continue;
+        if (best < 0 || st.total_ms < bst.total_ms) { best = i; bst = st; }
+    }
+    if (best < 0) return -1; /* the error of the last trial is kept */
+    t->tuned = c[best];
+    t->tuned_units = nunits;
+    t->tuned_ok = 1;
+    if (chosen) *chosen = c[best];
+    if (stats) *stats = bst;
+    /* the buffer holds the labels of the last trial: every trial writes the same bytes */
+    return 0;
+}
+
 /* The labeling call.  Chunk seeds come either from the session seed (derived
  * per super-chunk from its absolute position), or, when raw_seeds is set, are
  * taken as given: raw_seeds holds 32 bytes per super-chunk of the buffer. */
@@ -557,6 +628,7 @@ static int topo_label_core(const pose_hbm_topo_t *ct, const uint8_t *session_see
 
     const uint64_t per_launch = num_super < PB_MAX_CHUNKS_PER_LAUNCH ? num_super : PB_MAX_CHUNKS_PER_LAUNCH;
     plan_t plan;
+    if (!sched && t->tuned_ok && t->tuned_units == per_launch * t->copies) sched = &t->tuned;
     if (make_plan(t, per_launch * t->copies, sched, scratch_budget(t, sched), &plan) != 0) {
         set_err("pose_graph_hbm_topo_label: no schedule fits the scratch budget "
                 "(one copy needs %llu bytes)", (unsigned long long)t->pool * 32ull);

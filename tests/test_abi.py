@@ -49,6 +49,11 @@ def test_null_topology(pkg):
     L.pose_graph_hbm_topo_free(None)  # no-op, as in the reference
 
 
+def test_autotune_rejects_null_topology_and_short_buffer(pkg):
+    L = pkg.load()
+    assert L.pose_b200_topo_autotune(None, None, 0, None, 1 << 20, 0, 2, None, None) == -1
+
+
 def test_kat_rejects_null_arguments(pkg):
     L = pkg.load()
     out = (C.c_uint8 * 32)()

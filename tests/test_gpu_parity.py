@@ -121,6 +121,33 @@ def test_pipelined_kernel_with_few_teams(pkg, cuda, oracle):
         assert got == oracle.label_region(key, cb, 5, cb * 11, threads=8).tobytes(), cb
 
 
+def test_autotune_keeps_the_bytes_and_its_schedule(pkg, cuda, wl):
+    g = golden("configs.json")["plain_small"]
+    c = wl.plain_small()
+    n = c["chunks"] * c["chunk_blocks"] * 32
+    buf = dev_buffer(cuda, n)
+    with pkg.Topology(c["chunk_blocks"]) as topo:
+        rc, chosen, st = topo.autotune(c["key"], buf.data_ptr(), n, c["rbo"], trials=6)
+        assert rc == 0, pkg.last_error()
+        cuda.cuda.synchronize()
+        assert hashlib.sha256(host_bytes(buf)).hexdigest() == g["region_sha256"]
+        assert st["kernel"] == chosen["kernel"] and st["team_warps"] == chosen["team_warps"]
+        buf.fill_(0)
+        rc, st2 = topo.label(c["key"], buf.data_ptr(), n, c["rbo"], stats=True)
+        assert rc == 0, pkg.last_error()
+        assert (st2["kernel"], st2["team_warps"], st2["units_per_team"]) == \
+            (chosen["kernel"], chosen["team_warps"], chosen["units_per_team"])
+        assert hashlib.sha256(host_bytes(buf)).hexdigest() == g["region_sha256"]
+        # another call size keeps the automatic policy and the same bytes
+        buf.fill_(0)
+        half, sb = c["chunks"] // 2, c["chunk_blocks"] * 32
+        rc, st3 = topo.label(c["key"], buf.data_ptr(), half * sb, c["rbo"], stats=True)
+        assert rc == 0, pkg.last_error()
+        got = host_bytes(buf)
+        for j in range(half):
+            assert hashlib.sha256(got[j * sb:(j + 1) * sb]).hexdigest() == g["super_chunk_sha256"][j], j
+
+
 def test_few_resident_teams_loop_over_the_queue(pkg, cuda, wl):
     # 128 units through 3 resident teams: every team pulls many batches
     g = golden("configs.json")["plain_small"]
