@@ -211,7 +211,7 @@ def run_window(pkg, torch, topo, rate: float, reps: int = 1) -> dict:
     buf = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
     # warm-up: the timed-trial autotuner picks this window's schedule, which
     # the timed pose_graph_hbm_topo_label calls below then use
-    rc, chosen, _ = topo.autotune(w["key"], buf.data_ptr(), nbytes, 0, trials=4)
+    rc, chosen, _ = topo.autotune(w["key"], buf.data_ptr(), nbytes, 0, trials=10)
     assert rc == 0, pkg.last_error()
     best = None
     for _ in range(reps):
@@ -227,7 +227,7 @@ def run_window(pkg, torch, topo, rate: float, reps: int = 1) -> dict:
             "value": nbytes / MIB / (best["total_ms"] * 1e-3), "unit": "MiB/s", "ms": best["total_ms"],
             "kernel_ms": best["kernel_ms"], "kernel": best["kernel"],
             "schedule": {"T": best["team_warps"], "G": best["units_per_team"], "teams": best["teams"],
-                         "chosen_by": "pose_b200_topo_autotune (4 timed trials)"},
+                         "chosen_by": "pose_b200_topo_autotune (10 timed trials)"},
             "roofline": {"bound": "int32", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s",
                          "frac": achieved / peak,
                          "frac_of_spec_method": best["nodes"] * 3 * 680.0 / (best["kernel_ms"] * 1e-3) / peak}}

@@ -72,11 +72,14 @@ int pose_b200_plan(const pose_hbm_topo_t *topo, uint64_t super_chunks,
 
 /* Timed-trial autotuner for one call shape.  It has no counterpart in the
  * reference; it tunes pose_graph_hbm_topo_label (common/include/gpu_label.h:
- * 80-83).  It ranks the modelled best schedule of every team size of the
- * basic kernel and the depth kernel, runs the `trials` cheapest of them
- * (0 = 4) as real labeling calls on the given buffer, and remembers the
- * fastest: later calls on this topology with the same number of super-chunks
- * and no explicit schedule use it.  The buffer ends up holding the labels,
+ * 80-83).  It plans every (team size, units per team) of the basic kernel
+ * and the depth kernel with the schedule model and runs up to `trials`
+ * (0 = 4) of them as real labeling calls on the given buffer: first the
+ * modelled best of each team size and the depth kernel, then the other
+ * units-per-team choices of the fastest team size; candidates modelled at
+ * more than twice the cheapest are not run.  It remembers the
+ * fastest: later calls on this topology with the same number of
+ * super-chunks and no explicit schedule use it.  The buffer ends up holding the labels,
  * exactly as after pose_graph_hbm_topo_label.  Returns 0, or -1 on error;
  * `chosen` (may be NULL) gets the winning schedule and `stats` (may be NULL)
  * its timed call.  Same threading rule as the labeling call. */

@@ -527,29 +527,45 @@ static int topo_label_core(const pose_hbm_topo_t *ct, const uint8_t *session_see
                            const uint8_t *raw_seeds, void *hbm_dev_ptr, size_t hbm_len, uint64_t rbo,
                            const pose_b200_sched_t *sched, pose_b200_stats_t *stats);
 
-/* Candidates of the autotuner: the modelled best schedule of every team size
- * of the basic kernel and the depth kernel, cheapest model cost first. */
-static int autotune_candidates(pose_hbm_topo_t *t, uint64_t nunits, uint64_t budget, pose_b200_sched_t *c,
-                               double *cost, int max)
+/* Candidates of the autotuner: every (team size, units per team) of the
+ * basic kernel, and the depth kernel, as planned by the schedule model;
+ * group g = team size (0 = the depth kernel), cost = modelled cost. */
+#define PB_TUNE_MAX 40
+typedef struct {
+    pose_b200_sched_t s;
+    double cost;
+    uint32_t group;
+} tune_cand_t;
+
+static int autotune_candidates(pose_hbm_topo_t *t, uint64_t nunits, uint64_t budget, tune_cand_t *c)
 {
     int n = 0;
-    for (uint32_t k = 0; k < 6 && n < max; k++) {
-        pose_b200_sched_t h;
-        memset(&h, 0, sizeof(h));
-        if (k < 5) { h.kernel = 1; h.team_warps = 1u << k; }
-        else h.kernel = 3;
-        plan_t p;
-        if (make_plan(t, nunits, &h, budget, &p) != 0) continue;
-        pose_b200_sched_t s;
-        memset(&s, 0, sizeof(s));
-        s.kernel = p.kernel;
-        s.team_warps = p.T;
-        s.units_per_team = p.G;
-        s.max_teams = p.teams;
-        int i = n++;
-        while (i > 0 && cost[i - 1] > p.cost) { c[i] = c[i - 1]; cost[i] = cost[i - 1]; i--; }
-        c[i] = s;
-        cost[i] = p.cost;
+    for (uint32_t T = 1; T <= 16; T <<= 1)
+        for (uint32_t G = 1; G <= 32 && n < PB_TUNE_MAX - 1; G <<= 1) {
+            pose_b200_sched_t h;
+            memset(&h, 0, sizeof(h));
+            h.kernel = 1; h.team_warps = T; h.units_per_team = G;
+            plan_t p;
+            if (make_plan(t, nunits, &h, budget, &p) != 0) continue;
+            memset(&c[n], 0, sizeof(c[n]));
+            c[n].s.kernel = 1; c[n].s.team_warps = p.T; c[n].s.units_per_team = p.G; c[n].s.max_teams = p.teams;
+            c[n].cost = p.cost; c[n].group = T; n++;
+        }
+    pose_b200_sched_t h;
+    memset(&h, 0, sizeof(h));
+    h.kernel = 3;
+    plan_t p;
+    if (make_plan(t, nunits, &h, budget, &p) == 0) {
+        memset(&c[n], 0, sizeof(c[n]));
+        c[n].s.kernel = 3; c[n].s.team_warps = p.T; c[n].s.units_per_team = 1; c[n].s.max_teams = p.teams;
+        c[n].cost = p.cost; c[n].group = 0; n++;
+    }
+    /* by modelled cost */
+    for (int i = 1; i < n; i++) {
+        tune_cand_t v = c[i];
+        int j = i;
+        while (j > 0 && c[j - 1].cost > v.cost) { c[j] = c[j - 1]; j--; }
+        c[j] = v;
     }
     return n;
 }
@@ -564,27 +580,46 @@ int pose_b200_topo_autotune(pose_hbm_topo_t *t, const uint8_t *session_seed, siz
     if (num_super == 0) { set_err("pose_b200_topo_autotune: buffer smaller than one super-chunk"); return -1; }
     const uint64_t per_launch = num_super < PB_MAX_CHUNKS_PER_LAUNCH ? num_super : PB_MAX_CHUNKS_PER_LAUNCH;
     const uint64_t nunits = per_launch * t->copies;
-    pose_b200_sched_t c[6];
-    double cost[6];
+    tune_cand_t c[PB_TUNE_MAX];
+    int tried[PB_TUNE_MAX];
     t->tuned_ok = 0;
-    const int n = autotune_candidates(t, nunits, scratch_budget(t, NULL), c, cost, 6);
+    const int n = autotune_candidates(t, nunits, scratch_budget(t, NULL), c);
     if (n <= 0) { set_err("pose_b200_topo_autotune: no schedule fits the scratch budget"); return -1; }
-    const int k = (int)(trials == 0 ? 4u : trials) < n ? (int)(trials == 0 ? 4u : trials) : n;
+    memset(tried, 0, sizeof(tried));
+    int budget_trials = (int)(trials == 0 ? 4u : trials);
     int best = -1;
     pose_b200_stats_t bst;
     memset(&bst, 0, sizeof(bst));
-    for (int i = 0; i < k; i++) {
-        pose_b200_stats_t st;
-        if (topo_label_core(t, session_seed, seed_len, NULL, hbm_dev_ptr, hbm_len, region_block_offset, &c[i],
-                            &st) != 0)
-            continue;
-        if (best < 0 || st.total_ms < bst.total_ms) { best = i; bst = st; }
+    /* stage 1: the cheapest candidate of each group (team size or the depth
+     * kernel), cheapest first; stage 2: the other candidates of the winning
+     * group, cheapest first, with the trials left */
+    for (int stage = 0; stage < 2 && budget_trials > 0; stage++) {
+        uint32_t seen = 0; /* bit per group in stage 1 */
+        const uint32_t win = best >= 0 ? c[best].group : 0xFFFFFFFFu;
+        for (int i = 0; i < n && budget_trials > 0; i++) {
+            if (tried[i]) continue;
+            if (c[i].cost > 2.0 * c[0].cost) break; /* the model is good to well within 2x */
+            if (stage == 0) {
+                const uint32_t bit = 1u << (c[i].group ? __builtin_ctz(c[i].group) + 1 : 0);
+                if (seen & bit) continue;
+                seen |= bit;
+            } else if (c[i].group != win) {
+                continue;
+            }
+            tried[i] = 1;
+            budget_trials--;
+            pose_b200_stats_t st;
+            if (topo_label_core(t, session_seed, seed_len, NULL, hbm_dev_ptr, hbm_len, region_block_offset,
+                                &c[i].s, &st) != 0)
+                continue;
+            if (best < 0 || st.total_ms < bst.total_ms) { best = i; bst = st; }
+        }
     }
     if (best < 0) return -1; /* the error of the last trial is kept */
-    t->tuned = c[best];
+    t->tuned = c[best].s;
     t->tuned_units = nunits;
     t->tuned_ok = 1;
-    if (chosen) *chosen = c[best];
+    if (chosen) *chosen = c[best].s;
     if (stats) *stats = bst;
     /* the buffer holds the labels of the last trial: every trial writes the same bytes */
     return 0;
