@@ -17,6 +17,7 @@
  *     demand) and zeroed at the end of every call and before it is freed.
  */
 #include "b3_host.h"
+#include "dev_alloc.h"
 #include "kernels.h"
 #include "topology.h"
 
@@ -25,6 +26,7 @@
 
 #include <cuda_runtime_api.h>
 #include <math.h>
+#include <pthread.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -299,13 +301,39 @@ static int make_plan(const pose_hbm_topo_t *ct, uint64_t nunits, const pose_b200
         }                                                                                \
     } while (0)
 
+static pthread_mutex_t g_fail_mu = PTHREAD_MUTEX_INITIALIZER;
+static char g_fail_seen[32];
+static long g_fail_left;
+
+cudaError_t pb_dev_malloc(void **ptr, size_t bytes)
+{
+    const char *e = getenv("POSE_B200_FAIL_ALLOC");
+    pthread_mutex_lock(&g_fail_mu);
+    if (!e) e = "";
+    if (strncmp(e, g_fail_seen, sizeof(g_fail_seen) - 1) != 0) {
+        snprintf(g_fail_seen, sizeof(g_fail_seen), "%s", e);
+        g_fail_left = atol(e);
+    }
+    const int fail = g_fail_left > 0;
+    if (fail) g_fail_left--;
+    pthread_mutex_unlock(&g_fail_mu);
+    if (fail) {
+        *ptr = NULL;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(ptr, bytes);
+}
+
+static cudaError_t g_last_alloc_err; /* the error of the last failed grow() */
+
 static int grow(void **p, uint64_t *have, uint64_t need, size_t elem)
 {
     if (*have >= need) return 0;
     if (*p) cudaFree(*p);
     *p = NULL;
     *have = 0;
-    if (cudaMalloc(p, need * elem) != cudaSuccess) { *p = NULL; return -1; }
+    const cudaError_t e = pb_dev_malloc(p, need * elem);
+    if (e != cudaSuccess) { *p = NULL; g_last_alloc_err = e; return -1; }
     *have = need;
     return 0;
 }
@@ -402,10 +430,10 @@ pose_hbm_topo_t *pose_b200_topo_build(uint32_t chunk_blocks, int with_cv0_table)
     {
         CK(cudaStreamCreate(&t->stream), "stream");
         for (int i = 0; i < 4; i++) CK(cudaEventCreate(&t->ev[i]), "event");
-        CK(cudaMalloc(&t->d_recs, (size_t)h.S * 16), "topology records");
-        CK(cudaMalloc(&t->d_orank, (size_t)h.S * 4), "output ranks");
-        CK(cudaMalloc(&t->d_lstart, ((size_t)h.L + 1) * 4), "level offsets");
-        CK(cudaMalloc((void **)&t->d_queue, 64), "work counter");
+        CK(pb_dev_malloc(&t->d_recs, (size_t)h.S * 16), "topology records");
+        CK(pb_dev_malloc(&t->d_orank, (size_t)h.S * 4), "output ranks");
+        CK(pb_dev_malloc(&t->d_lstart, ((size_t)h.L + 1) * 4), "level offsets");
+        CK(pb_dev_malloc((void **)&t->d_queue, 64), "work counter");
         t->dev_bytes = (uint64_t)h.S * 20 + ((uint64_t)h.L + 1) * 4;
         CK(cudaMemcpyAsync(t->d_recs, h.recs, (size_t)h.S * 16, cudaMemcpyHostToDevice, t->stream),
            "upload records");
@@ -422,14 +450,14 @@ pose_hbm_topo_t *pose_b200_topo_build(uint32_t chunk_blocks, int with_cv0_table)
             goto fail;
         }
         if (with_cv0_table && h.recs2) {
-            CK(cudaMalloc(&t->d_recs2, (size_t)h.S * 32), "pipelined records");
+            CK(pb_dev_malloc(&t->d_recs2, (size_t)h.S * 32), "pipelined records");
             CK(cudaMemcpyAsync(t->d_recs2, h.recs2, (size_t)h.S * 32, cudaMemcpyHostToDevice, t->stream),
                "upload pipelined records");
             t->dev_bytes += (uint64_t)h.S * 32;
         }
         if (with_cv0_table) {
             uint64_t bytes = (uint64_t)t->copies * h.S * 32;
-            CK(cudaMalloc(&t->d_cv0, bytes), "block-0 table");
+            CK(pb_dev_malloc(&t->d_cv0, bytes), "block-0 table");
             t->dev_bytes += bytes;
             if (pb_dev_cv0_table(t->d_recs, h.S, t->copies, t->d_cv0, t->stream) != 0) {
                 set_err("pose_graph_hbm_topo_build: block-0 table kernel failed");
@@ -664,10 +692,29 @@ static int topo_label_core(const pose_hbm_topo_t *ct, const uint8_t *session_see
     const uint64_t per_launch = num_super < PB_MAX_CHUNKS_PER_LAUNCH ? num_super : PB_MAX_CHUNKS_PER_LAUNCH;
     plan_t plan;
     if (!sched && t->tuned_ok && t->tuned_units == per_launch * t->copies) sched = &t->tuned;
-    if (make_plan(t, per_launch * t->copies, sched, scratch_budget(t, sched), &plan) != 0) {
+    uint64_t budget = scratch_budget(t, sched);
+    if (make_plan(t, per_launch * t->copies, sched, budget, &plan) != 0) {
         set_err("pose_graph_hbm_topo_label: no schedule fits the scratch budget "
                 "(one copy needs %llu bytes)", (unsigned long long)t->pool * 32ull);
         goto out;
+    }
+    /* scratch: when the allocation fails, halve the budget and re-plan, down
+     * to a single team, as the reference halves its chunk batch on an
+     * allocation failure (common/src/cuda/label_gpu_warp.cu:165-175) */
+    while (grow((void **)&t->d_scratch, &t->scratch_alloc, plan.scratch_bytes, 1) != 0) {
+        cudaGetLastError();
+        if (plan.scratch_bytes <= plan.team_scratch || plan.teams <= 1) {
+            set_err("pose_graph_hbm_topo_label: scratch alloc of %llu bytes failed: %s",
+                    (unsigned long long)plan.scratch_bytes, cudaGetErrorString(g_last_alloc_err));
+            goto out;
+        }
+        budget = plan.scratch_bytes / 2;
+        if (budget < plan.team_scratch) budget = plan.team_scratch;
+        if (make_plan(t, per_launch * t->copies, sched, budget, &plan) != 0) {
+            set_err("pose_graph_hbm_topo_label: no schedule fits %llu bytes of scratch",
+                    (unsigned long long)budget);
+            goto out;
+        }
     }
     if (!quiet()) {
         printf("  GPU label: strategy=b200  %llu super-chunks  scaffold=%llu nodes  "
@@ -677,11 +724,6 @@ static int topo_label_core(const pose_hbm_topo_t *ct, const uint8_t *session_see
     }
     {
         double t0 = now_sec();
-        if (grow((void **)&t->d_scratch, &t->scratch_alloc, plan.scratch_bytes, 1) != 0) {
-            set_err("pose_graph_hbm_topo_label: scratch alloc of %llu bytes failed",
-                    (unsigned long long)plan.scratch_bytes);
-            goto out;
-        }
         if (grow((void **)&t->d_seeds, &t->seeds_alloc, per_launch, 32) != 0) {
             set_err("pose_graph_hbm_topo_label: seed buffer alloc failed");
             goto out;
@@ -885,7 +927,7 @@ int pose_gpu_label_node_single(uint8_t out[32], int is_source, uint64_t node_ind
     memcpy(in + 40, key_int, 32);
     uint32_t *d = NULL, res[8];
     int rc = -1;
-    CK(cudaMalloc((void **)&d, sizeof(in)), "KAT alloc");
+    CK(pb_dev_malloc((void **)&d, sizeof(in)), "KAT alloc");
     CK(cudaMemcpy(d, in, sizeof(in), cudaMemcpyHostToDevice), "KAT upload");
     if (pb_dev_label_single(d + 48, is_source, node_index, d, pred0 != NULL, pred1 != NULL, 0) != 0) {
         set_err("pose_gpu_label_node_single: launch failed");
@@ -916,8 +958,8 @@ double pose_b200_compress_rate(uint32_t iters, double *latency_cycles)
     double rate = 0;
     cudaGetDevice(&dev);
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-    CK(cudaMalloc((void **)&d_sink, 4096 * 4), "sink");
-    CK(cudaMalloc((void **)&d_cyc, 8), "cycles");
+    CK(pb_dev_malloc((void **)&d_sink, 4096 * 4), "sink");
+    CK(pb_dev_malloc((void **)&d_cyc, 8), "cycles");
     CK(cudaEventCreate(&a), "event");
     CK(cudaEventCreate(&b), "event");
     {

@@ -22,6 +22,7 @@
  *     zeroing are captured once into a CUDA graph and replayed.
  */
 #include "batch_internal.h"
+#include "dev_alloc.h"
 #include "kernels.h"
 #include "topo_internal.h"
 #include "pose_b200.h"
@@ -376,14 +377,14 @@ pose_b200_batch_t *pose_b200_batch_create(const pose_b200_request_t *reqs, size_
 
         BK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream");
         for (int i = 0; i < 4; i++) BK(cudaEventCreate(&b->ev[i]), "event");
-        BK(cudaMalloc(&b->d_topos, pl.ntopo * sizeof(pb_topo_view_t)), "alloc");
-        BK(cudaMalloc(&b->d_batches, pl.nbatches * sizeof(pb_mbatch_t)), "alloc");
-        BK(cudaMalloc(&b->d_units, pl.nunits * sizeof(pb_munit_t)), "alloc");
-        BK(cudaMalloc(&b->d_jobs, pl.njobs * sizeof(pb_seedjob_t)), "alloc");
-        BK(cudaMalloc(&b->d_blob, blob_len ? blob_len : 1), "alloc");
-        BK(cudaMalloc(&b->d_seeds, pl.njobs * 32), "alloc");
-        BK(cudaMalloc(&b->d_scratch, b->scratch_bytes), "scratch alloc");
-        BK(cudaMalloc(&b->d_queue, 64), "alloc");
+        BK(pb_dev_malloc(&b->d_topos, pl.ntopo * sizeof(pb_topo_view_t)), "alloc");
+        BK(pb_dev_malloc(&b->d_batches, pl.nbatches * sizeof(pb_mbatch_t)), "alloc");
+        BK(pb_dev_malloc(&b->d_units, pl.nunits * sizeof(pb_munit_t)), "alloc");
+        BK(pb_dev_malloc(&b->d_jobs, pl.njobs * sizeof(pb_seedjob_t)), "alloc");
+        BK(pb_dev_malloc(&b->d_blob, blob_len ? blob_len : 1), "alloc");
+        BK(pb_dev_malloc(&b->d_seeds, pl.njobs * 32), "alloc");
+        BK(pb_dev_malloc(&b->d_scratch, b->scratch_bytes), "scratch alloc");
+        BK(pb_dev_malloc(&b->d_queue, 64), "alloc");
         BK(cudaMemcpyAsync(b->d_topos, pl.views, pl.ntopo * sizeof(pb_topo_view_t), cudaMemcpyHostToDevice, b->stream), "upload");
         BK(cudaMemcpyAsync(b->d_batches, pl.batches, pl.nbatches * sizeof(pb_mbatch_t), cudaMemcpyHostToDevice, b->stream), "upload");
         BK(cudaMemcpyAsync(b->d_units, pl.units, pl.nunits * sizeof(pb_munit_t), cudaMemcpyHostToDevice, b->stream), "upload");

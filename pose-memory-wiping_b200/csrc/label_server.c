@@ -24,6 +24,7 @@
  * Every request's bytes are those of labelling it alone.
  */
 #include "batch_internal.h"
+#include "dev_alloc.h"
 #include "kernels.h"
 #include "pose_b200.h"
 
@@ -241,7 +242,7 @@ static int admit(pose_b200_server_t *s)
         cudaFree(wv->d_tables);
         wv->d_tables = NULL;
         wv->tables_cap = 0;
-        if (cudaMalloc(&wv->d_tables, total * 2) != cudaSuccess) { arena_give(s, off, scratch); pb_plan_free(&pl); return 0; }
+        if (pb_dev_malloc(&wv->d_tables, total * 2) != cudaSuccess) { arena_give(s, off, scratch); pb_plan_free(&pl); return 0; }
         wv->tables_cap = total * 2;
     }
     uint8_t *T = (uint8_t *)wv->d_tables;
@@ -376,7 +377,7 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
         scratch_bytes = fr > ((uint64_t)8 << 30) ? (uint64_t)(fr / 2) : (uint64_t)(fr / 4);
     }
     scratch_bytes &= ~(uint64_t)255;
-    if (cudaMalloc((void **)&s->d_arena, scratch_bytes) != cudaSuccess) {
+    if (pb_dev_malloc((void **)&s->d_arena, scratch_bytes) != cudaSuccess) {
         fprintf(stderr, "pose_b200_server_create: scratch arena of %llu bytes failed\n", (unsigned long long)scratch_bytes);
         goto fail;
     }
@@ -426,7 +427,7 @@ int pose_b200_server_session(pose_b200_server_t *s, const uint8_t *seed, size_t 
         size_t ncap = (s->sess_cap ? s->sess_cap * 2 : 4096);
         while (ncap < s->sess_bytes + seed_len) ncap *= 2;
         uint8_t *nb = NULL;
-        if (cudaMalloc((void **)&nb, ncap) != cudaSuccess) goto out;
+        if (pb_dev_malloc((void **)&nb, ncap) != cudaSuccess) goto out;
         if (s->sess_bytes && cudaMemcpy(nb, s->d_sessions, s->sess_bytes, cudaMemcpyDeviceToDevice) != cudaSuccess) {
             cudaFree(nb);
             goto out;

@@ -13,6 +13,7 @@
  * there, may be called from a worker thread.
  */
 #include "pose_b200.h"
+#include "dev_alloc.h"
 
 #include <cuda_runtime_api.h>
 #include <pthread.h>
@@ -124,7 +125,7 @@ int pose_b200_label_stream(const pose_hbm_topo_t *topo, const uint8_t *session_s
     memset(&last, 0, sizeof(last));
 
     for (int i = 0; i < 2; i++) {
-        if (cudaMalloc((void **)&s.dev[i], wbytes) != cudaSuccess ||
+        if (pb_dev_malloc((void **)&s.dev[i], wbytes) != cudaSuccess ||
             cudaMallocHost((void **)&s.host[i], wbytes) != cudaSuccess) {
             fprintf(stderr, "pose_b200_label_stream: window buffers of %llu bytes failed\n",
                     (unsigned long long)wbytes);

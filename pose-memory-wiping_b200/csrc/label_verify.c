@@ -14,6 +14,7 @@
  * device while the next group's reads are already done.
  */
 #include "kernels.h"
+#include "dev_alloc.h"
 #include "pose_b200.h"
 #include "topo_internal.h"
 
@@ -64,7 +65,7 @@ int pose_b200_challenge(const pose_hbm_topo_t *topo, const uint8_t *seed, size_t
     if (prev != ti.device && cudaSetDevice(ti.device) != cudaSuccess) return -1;
     int rc = -1;
     void *buf = NULL;
-    if (cudaMalloc(&buf, ti.super_bytes) != cudaSuccess) {
+    if (pb_dev_malloc(&buf, ti.super_bytes) != cudaSuccess) {
         fprintf(stderr, "pose_b200_challenge: %s\n", cudaGetErrorString(cudaGetLastError()));
         goto out;
     }
@@ -157,9 +158,9 @@ int pose_b200_challenge_blocks(const pose_hbm_topo_t *topo, const uint8_t *sessi
         for (size_t i = 0; i < n; i++)
             if (i == 0 || c[i].chunk != c[i - 1].chunk) distinct++;
         const uint64_t wchunks = distinct < group_cap ? distinct : group_cap;
-        if (cudaMalloc((void **)&d_work, wchunks * ti.super_bytes) != cudaSuccess ||
-            cudaMalloc((void **)&d_out, n * 32) != cudaSuccess ||
-            cudaMalloc((void **)&d_src, n * sizeof(uint64_t)) != cudaSuccess) {
+        if (pb_dev_malloc((void **)&d_work, wchunks * ti.super_bytes) != cudaSuccess ||
+            pb_dev_malloc((void **)&d_out, n * 32) != cudaSuccess ||
+            pb_dev_malloc((void **)&d_src, n * sizeof(uint64_t)) != cudaSuccess) {
             fprintf(stderr, "pose_b200_challenge_blocks: device allocation failed: %s\n",
                     cudaGetErrorString(cudaGetLastError()));
             goto out;
@@ -282,9 +283,9 @@ int pose_b200_verify_sampled(const pose_hbm_topo_t *topo, const uint8_t *session
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMallocHost((void **)&h_disk, group * sb) != cudaSuccess ||
         cudaMallocHost((void **)&h_bad, group * sizeof(unsigned long long)) != cudaSuccess ||
-        cudaMalloc((void **)&d_disk, group * sb) != cudaSuccess ||
-        cudaMalloc((void **)&d_ref, group * sb) != cudaSuccess ||
-        cudaMalloc((void **)&d_bad, group * sizeof(unsigned long long)) != cudaSuccess) {
+        pb_dev_malloc((void **)&d_disk, group * sb) != cudaSuccess ||
+        pb_dev_malloc((void **)&d_ref, group * sb) != cudaSuccess ||
+        pb_dev_malloc((void **)&d_bad, group * sizeof(unsigned long long)) != cudaSuccess) {
         fprintf(stderr, "pose_b200_verify_sampled: buffers of %llu bytes failed: %s\n",
                 (unsigned long long)(group * sb), cudaGetErrorString(cudaGetLastError()));
         goto out;
