@@ -263,7 +263,7 @@ def run_batched(pkg, torch, sched=None, reps: int = 2) -> dict:
             "value": total / MIB / (best["total_ms"] * 1e-3), "unit": "MiB/s",
             "graph_ms": best["total_ms"], "super_chunks": best["super_chunks"], "units": best["units"],
             "nodes": best["nodes"], "teams": best["teams"], "team_warps": best["team_warps"],
-            "max_units_per_team": best["units_per_team"], "kernel_launches_per_replay": 2,
+            "max_units_per_team": best["units_per_team"], "kernel_launches_per_replay": best["kernel_launches"],
             "schedule": "autotuned" if chosen else "given",
             "packing": None if not chosen else ("chain-bounded" if chosen["lane_efficiency"] == pkg.PACK_CHAIN
                                                  else f"lane efficiency {chosen['lane_efficiency']}%")}

@@ -29,10 +29,14 @@ typedef struct {
     uint32_t lane_efficiency;   /* batched launches: per-topology G reaches this lane efficiency,
                                    in percent; POSE_B200_PACK_CHAIN packs units while their chain
                                    stays within the launch's longest; 0 = automatic */
-    uint32_t reserved;
+    uint32_t flags;             /* POSE_B200_BATCH_* (batched launches); 0 otherwise */
 } pose_b200_sched_t;
 
 #define POSE_B200_PACK_CHAIN 255u
+/* flags: run every request of a batch in one launch.  Without it, a batch
+ * whose deepest topologies are much deeper than the rest runs them as a
+ * second, concurrent launch of 8-warp teams. */
+#define POSE_B200_BATCH_ONE_LAUNCH 1u
 
 /* What one call did (device times from CUDA events on the labeler's stream). */
 typedef struct {
@@ -118,7 +122,12 @@ typedef struct pose_b200_batch pose_b200_batch_t;
  * their buffers must stay valid until the batch is destroyed.  sched may fix
  * team_warps (1, 2, 4 or 8) and lane_efficiency, and cap units_per_team (the
  * largest G), max_teams and scratch_cap_bytes; what it leaves at 0 is chosen
- * by the makespan estimate. */
+ * by the makespan estimate.  Deep part: the requests whose topology's chain
+ * (passes of an 8-warp team over one chunk copy) is at least 3/4 of the
+ * deepest, when the others are shallower, run as a second launch captured
+ * beside the first (8-warp teams, units packed up to 4 a team so that they
+ * hold about half the SMs' team slots) unless flags has
+ * POSE_B200_BATCH_ONE_LAUNCH; sched then applies to the rest. */
 pose_b200_batch_t *pose_b200_batch_create(const pose_b200_request_t *reqs, size_t n,
                                           const pose_b200_sched_t *sched);
 /* The empirical autotuner: rank the schedules sched leaves open (team size

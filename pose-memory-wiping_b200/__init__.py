@@ -38,10 +38,11 @@ class Sched(C.Structure):
     _fields_ = [("team_warps", C.c_uint32), ("units_per_team", C.c_uint32),
                 ("max_teams", C.c_uint32), ("kernel", C.c_uint32),
                 ("scratch_cap_bytes", C.c_uint64), ("lane_efficiency", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("flags", C.c_uint32)]
 
 
 PACK_CHAIN = 255  # POSE_B200_PACK_CHAIN: pack units while their chain stays within the launch's longest
+BATCH_ONE_LAUNCH = 1  # POSE_B200_BATCH_ONE_LAUNCH (Sched.flags): no separate launch for the deepest requests
 
 
 class Stats(C.Structure):

@@ -55,7 +55,7 @@ def test_batch_equals_individual_calls(pkg, cuda, oracle):
 
 @pytest.mark.parametrize("sched", [None, {"team_warps": 2, "units_per_team": 4}, {"max_teams": 5},
                                    {"team_warps": 8, "lane_efficiency": 255}, {"team_warps": 1, "lane_efficiency": 70},
-                                   {"team_warps": 4, "units_per_team": 1}, "autotune"])
+                                   {"team_warps": 4, "units_per_team": 1}, {"flags": 1}, "autotune"])
 def test_batch_schedules(pkg, cuda, oracle, sched):
     topos = {cb: pkg.Topology(cb) for cb in (64, 512)}
     try:
@@ -77,6 +77,35 @@ def test_batch_schedules(pkg, cuda, oracle, sched):
         for (topo, key, _, nbytes, rbo), buf in zip(reqs, bufs):
             want = oracle.label_region(key, topo.chunk_blocks, 3, rbo, threads=4).tobytes()
             assert buf.cpu().numpy().tobytes() == want
+    finally:
+        for t in topos.values():
+            t.free()
+
+
+def test_deep_requests_run_as_a_second_launch(pkg, cuda):
+    """Requests of a much deeper topology run as their own concurrent launch;
+    POSE_B200_BATCH_ONE_LAUNCH keeps one launch; both write the same bytes."""
+    topos = {cb: pkg.Topology(cb) for cb in (256, 4096)}
+    try:
+        reqs, bufs = [], []
+        for i in range(10):
+            cb = 4096 if i < 3 else 256
+            buf = cuda.zeros(2 * cb * 32, dtype=cuda.uint8, device="cuda")
+            reqs.append((topos[cb], bytes([i + 7]) * 32, buf.data_ptr(), 2 * cb * 32, (5 + i) * cb))
+            bufs.append(buf)
+        got = {}
+        for flags, launches in ((0, 4), (pkg.BATCH_ONE_LAUNCH, 2)):
+            for t in bufs:
+                t.fill_(0x33)
+            with pkg.Batch(reqs, pkg.Sched(flags=flags)) as b:
+                rc, st = b.run()
+            assert rc == 0 and st["kernel_launches"] == launches, (flags, st)
+            got[flags] = [t.cpu().numpy().tobytes() for t in bufs]
+        assert got[0] == got[pkg.BATCH_ONE_LAUNCH]
+        for (topo, key, ptr, nbytes, rbo), data in zip(reqs, got[0]):
+            ref = cuda.zeros(nbytes, dtype=cuda.uint8, device="cuda")
+            assert topo.label(key, ref.data_ptr(), nbytes, rbo) == 0
+            assert ref.cpu().numpy().tobytes() == data
     finally:
         for t in topos.values():
             t.free()
