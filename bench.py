@@ -3,7 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                     [--workload plain_2e17|plain_small|window_2e17|throughput_2e12|
-                                latency_2e14|batched|served] [--no-aux] [--no-cpu-baseline]
+                                latency_2e14|deep_2e20|batched|served] [--no-aux] [--no-cpu-baseline]
 
 One step = one pass of the hot path over one batch: label the workload's
 super-chunks (default: 32 consecutive super-chunks at chunk_blocks = 2^17,
@@ -65,6 +65,9 @@ def workload(name: str) -> dict:
     elif name == "throughput_2e12":
         # profiling case: many chunks in flight, ~0.1 s kernel, scratch + store > L2
         w = dict(wl.plain_2e17(), name="throughput_2e12", chunk_blocks=1 << 12, chunks=2048)
+    elif name == "deep_2e20":
+        # deep-graph stress: 4 chunks at chunk_blocks 2^20, scratch capped at 40 GiB
+        w = wl.deep_2e20()
     elif name == "latency_2e14":
         # profiling case: few chunks, depth-bound, ~0.1 s kernel
         w = dict(wl.plain_2e17(), name="latency_2e14", chunk_blocks=1 << 14, chunks=16)
@@ -374,19 +377,22 @@ def run_b200(args) -> None:
     # roofline denominator: the GPU's compression rate for this instruction mix
     rate, lat_cycles = pkg.compress_rate(2048)
 
-    # warm-up: the timed-trial autotuner fixes this call size's schedule (the
-    # timed calls are plain pose_graph_hbm_topo_label calls that reuse it)
-    rc, _, _ = topo.autotune(w["key"], buf.data_ptr(), nbytes, rbo, trials=3)
-    assert rc == 0, pkg.last_error()
+    # a workload with a scratch cap runs every call under it; otherwise the
+    # timed-trial autotuner fixes this call size's schedule during warm-up
+    # (the timed calls are plain pose_graph_hbm_topo_label calls that reuse it)
+    cap = pkg.Sched(scratch_cap_bytes=w["scratch_cap_bytes"]) if w.get("scratch_cap_bytes") else None
+    if cap is None:
+        rc, _, _ = topo.autotune(w["key"], buf.data_ptr(), nbytes, rbo, trials=3)
+        assert rc == 0, pkg.last_error()
     for _ in range(args.warmup):
-        rc = topo.label(w["key"], buf.data_ptr(), nbytes, rbo)
+        rc = topo.label(w["key"], buf.data_ptr(), nbytes, rbo, sched=cap)
         assert rc == 0, pkg.last_error()
 
     stats = []
     barrier()
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
-            rc, st = topo.label(w["key"], buf.data_ptr(), nbytes, rbo, stats=True)
+            rc, st = topo.label(w["key"], buf.data_ptr(), nbytes, rbo, sched=cap, stats=True)
             assert rc == 0, pkg.last_error()
             stats.append(st)
         barrier()
@@ -397,7 +403,7 @@ def run_b200(args) -> None:
         for _ in range(max(1, args.steps)):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            rc = topo.label(w["key"], buf.data_ptr(), nbytes, rbo)
+            rc = topo.label(w["key"], buf.data_ptr(), nbytes, rbo, sched=cap)
             host.copy_(buf, non_blocking=False)
             torch.cuda.synchronize()
             e2e_times.append(time.perf_counter() - t0)
@@ -435,7 +441,9 @@ def run_b200(args) -> None:
         "config": {"workload": w["name"], "chunk_blocks": cb, "super_chunks": nsup,
                    "nodes_per_step": nsup * w["nodes_per_chunk"], "parallelism": f"chunk-sharded x{world}",
                    "l2": "inputs larger than L2 (topology store %.2f GB read per step)" % (info["device_bytes"] / 1e9),
-                   "schedule": {"T": st0["team_warps"], "G": st0["units_per_team"], "teams": st0["teams"]},
+                   "schedule": {"T": st0["team_warps"], "G": st0["units_per_team"], "teams": st0["teams"],
+                                "kernel": st0["kernel"], "scratch_bytes": st0["scratch_bytes"]},
+                   "scratch_cap_bytes": w.get("scratch_cap_bytes"),
                    "cv0_table": bool(st0["used_cv0_table"])},
         "roofline": {"bound": "int32", "achieved": achieved_ops / 1e12, "peak": peak_ops / 1e12,
                      "unit": "Tops/s", "frac": achieved_ops / peak_ops, "traffic": traffic,
