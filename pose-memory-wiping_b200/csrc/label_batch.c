@@ -312,20 +312,31 @@ int pb_plan_choose(const pb_req_t *pr, size_t n, const pose_b200_sched_t *sched,
 /* Requests whose topology's chain with 8-warp teams is at least 3/4 of the
  * deepest one's, when some other request's topology is shallower: they run
  * as their own launch beside the rest (1 = deep, 0 = rest, in deep[]).
- * Returns the number of deep requests (0 = no split). */
+ * Requests shorter than one super-chunk label nothing and stay with the
+ * rest.  Returns the number of deep requests (0 = no split). */
 static size_t split_deep(const pb_req_t *pr, size_t n, uint8_t *deep)
 {
-    uint64_t maxc = 0;
+    uint64_t maxc = 0, minc = UINT64_MAX;
     for (size_t i = 0; i < n; i++) {
+        pb_topo_internal_t x;
+        deep[i] = 0;
+        if (pb_topo_internal(pr[i].topo, &x) != 0 || pr[i].len < x.super_bytes) continue;
         const uint64_t c = pb_topo_passes(pr[i].topo, 8, 1);
         if (c > maxc) maxc = c;
+        if (c < minc) minc = c;
+        deep[i] = 1; /* has work; decided below */
+    }
+    if (maxc == 0 || 4 * minc >= 3 * maxc) {
+        memset(deep, 0, n);
+        return 0; /* every request with work is about as deep as the deepest */
     }
     size_t nd = 0;
     for (size_t i = 0; i < n; i++) {
+        if (!deep[i]) continue;
         deep[i] = 4 * pb_topo_passes(pr[i].topo, 8, 1) >= 3 * maxc;
         nd += deep[i];
     }
-    return nd == n ? 0 : nd;
+    return nd;
 }
 
 /* Size, allocate and upload one launch of a batch; `slots` caps its resident
@@ -505,8 +516,7 @@ no_split:
             }
             uint32_t g = 1;
             while (g < 4 && 2 * (dunits + g - 1) / g > (uint64_t)sms * occ) g *= 2;
-            if (pb_plan_requests(pd, nd, 8, g, 0.9999, &pl[1]) != 0) goto fail;
-            if (pl[1].nunits == 0) goto fail;
+            if (pb_plan_requests(pd, nd, 8, g, 0.9999, &pl[1]) != 0 || pl[1].nunits == 0) goto fail;
             deep_ctas = pl[1].nbatches;
             if (deep_ctas * 2 > (uint64_t)pl[1].sms * occ) deep_ctas = (uint64_t)pl[1].sms * occ / 2;
             if (part_setup(b, &b->part[1], &pl[1], 8, deep_ctas, budget, NULL) != 0) goto fail;

@@ -88,10 +88,11 @@ def test_deep_requests_run_as_a_second_launch(pkg, cuda):
     topos = {cb: pkg.Topology(cb) for cb in (256, 4096)}
     try:
         reqs, bufs = [], []
-        for i in range(10):
-            cb = 4096 if i < 3 else 256
-            buf = cuda.zeros(2 * cb * 32, dtype=cuda.uint8, device="cuda")
-            reqs.append((topos[cb], bytes([i + 7]) * 32, buf.data_ptr(), 2 * cb * 32, (5 + i) * cb))
+        for i in range(11):
+            cb = 4096 if i < 3 or i == 10 else 256
+            n = 2 * cb * 32 if i != 10 else 32  # the last: shorter than one super-chunk, labels nothing
+            buf = cuda.zeros(n, dtype=cuda.uint8, device="cuda")
+            reqs.append((topos[cb], bytes([i + 7]) * 32, buf.data_ptr(), n, (5 + i) * cb))
             bufs.append(buf)
         got = {}
         for flags, launches in ((0, 4), (pkg.BATCH_ONE_LAUNCH, 2)):
@@ -103,9 +104,13 @@ def test_deep_requests_run_as_a_second_launch(pkg, cuda):
             got[flags] = [t.cpu().numpy().tobytes() for t in bufs]
         assert got[0] == got[pkg.BATCH_ONE_LAUNCH]
         for (topo, key, ptr, nbytes, rbo), data in zip(reqs, got[0]):
-            ref = cuda.zeros(nbytes, dtype=cuda.uint8, device="cuda")
+            ref = cuda.full((nbytes,), 0x33, dtype=cuda.uint8, device="cuda")
             assert topo.label(key, ref.data_ptr(), nbytes, rbo) == 0
             assert ref.cpu().numpy().tobytes() == data
+        # only short deep requests: no deep part, nothing to label there
+        with pkg.Batch([reqs[10], reqs[5]]) as b:
+            rc, st = b.run()
+            assert rc == 0 and st["kernel_launches"] == 2
     finally:
         for t in topos.values():
             t.free()
