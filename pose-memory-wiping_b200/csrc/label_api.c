@@ -324,7 +324,7 @@ cudaError_t pb_dev_malloc(void **ptr, size_t bytes)
     return cudaMalloc(ptr, bytes);
 }
 
-static cudaError_t g_last_alloc_err; /* the error of the last failed grow() */
+static _Thread_local cudaError_t g_last_alloc_err; /* this thread's last failed grow() */
 
 static int grow(void **p, uint64_t *have, uint64_t need, size_t elem)
 {
