@@ -24,6 +24,7 @@
 #include "gpu_label.h"
 #include "pose_b200.h"
 
+#include <nvtx3/nvToolsExt.h>
 #include <cuda_runtime_api.h>
 #include <math.h>
 #include <pthread.h>
@@ -388,7 +389,7 @@ static int cmp_u32(const void *a, const void *b)
     return x < y ? -1 : x > y;
 }
 
-pose_hbm_topo_t *pose_b200_topo_build(uint32_t chunk_blocks, int with_cv0_table)
+static pose_hbm_topo_t *pose_b200_topo_build_impl(uint32_t chunk_blocks, int with_cv0_table)
 {
     uint32_t cb = chunk_blocks ? chunk_blocks : PB_DEFAULT_CHUNK_BLOCKS;
     if (cb > PB_MAX_CHUNK_BLOCKS) {
@@ -500,6 +501,14 @@ fail_host:
     pb_topo_host_free(&h);
     if (t) { free(t->wval); free(t->wcnt); free(t); }
     return NULL;
+}
+
+pose_hbm_topo_t *pose_b200_topo_build(uint32_t chunk_blocks, int with_cv0_table)
+{
+    nvtxRangePushA("pose_b200: topology build");
+    pose_hbm_topo_t *rc = pose_b200_topo_build_impl(chunk_blocks, with_cv0_table);
+    nvtxRangePop();
+    return rc;
 }
 
 pose_hbm_topo_t *pose_graph_hbm_topo_build(uint32_t chunk_blocks, pose_hash_algo_t algo)
@@ -656,7 +665,7 @@ int pose_b200_topo_autotune(pose_hbm_topo_t *t, const uint8_t *session_seed, siz
 /* The labeling call.  Chunk seeds come either from the session seed (derived
  * per super-chunk from its absolute position), or, when raw_seeds is set, are
  * taken as given: raw_seeds holds 32 bytes per super-chunk of the buffer. */
-static int topo_label_core(const pose_hbm_topo_t *ct, const uint8_t *session_seed, size_t seed_len,
+static int topo_label_core_impl(const pose_hbm_topo_t *ct, const uint8_t *session_seed, size_t seed_len,
                            const uint8_t *raw_seeds, void *hbm_dev_ptr, size_t hbm_len, uint64_t rbo,
                            const pose_b200_sched_t *sched, pose_b200_stats_t *stats)
 {
@@ -852,6 +861,16 @@ out:
         if (e != cudaSuccess) fprintf(stderr, "pose_graph_hbm_topo_label: CUDA error: %s\n", cudaGetErrorString(e));
     }
     if (prev >= 0 && prev != t->device) cudaSetDevice(prev);
+    return rc;
+}
+
+static int topo_label_core(const pose_hbm_topo_t *ct, const uint8_t *session_seed, size_t seed_len,
+                           const uint8_t *raw_seeds, void *hbm_dev_ptr, size_t hbm_len, uint64_t rbo,
+                           const pose_b200_sched_t *sched, pose_b200_stats_t *stats)
+{
+    nvtxRangePushA("pose_b200: label call");
+    int rc = topo_label_core_impl(ct, session_seed, seed_len, raw_seeds, hbm_dev_ptr, hbm_len, rbo, sched, stats);
+    nvtxRangePop();
     return rc;
 }
 

@@ -27,6 +27,7 @@
 #include "topo_internal.h"
 #include "pose_b200.h"
 
+#include <nvtx3/nvToolsExt.h>
 #include <cuda_runtime_api.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -581,7 +582,7 @@ fail_host:
     return NULL;
 }
 
-int pose_b200_batch_run(pose_b200_batch_t *b, pose_b200_stats_t *stats)
+static int pose_b200_batch_run_impl(pose_b200_batch_t *b, pose_b200_stats_t *stats)
 {
     if (stats) memset(stats, 0, sizeof(*stats));
     if (!b) return -1;
@@ -619,6 +620,14 @@ int pose_b200_batch_run(pose_b200_batch_t *b, pose_b200_stats_t *stats)
 out:
     if (rc != 0) fprintf(stderr, "pose_b200_batch_run: CUDA error: %s\n", cudaGetErrorString(cudaGetLastError()));
     if (prev >= 0 && prev != b->device) cudaSetDevice(prev);
+    return rc;
+}
+
+int pose_b200_batch_run(pose_b200_batch_t *b, pose_b200_stats_t *stats)
+{
+    nvtxRangePushA("pose_b200: batch replay");
+    int rc = pose_b200_batch_run_impl(b, stats);
+    nvtxRangePop();
     return rc;
 }
 

@@ -15,6 +15,7 @@
 #include "pose_b200.h"
 #include "dev_alloc.h"
 
+#include <nvtx3/nvToolsExt.h>
 #include <cuda_runtime_api.h>
 #include <pthread.h>
 #include <stdio.h>
@@ -89,7 +90,7 @@ static void *sink_worker(void *arg)
     return NULL;
 }
 
-int pose_b200_label_stream(const pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
+static int pose_b200_label_stream_impl(const pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
                            uint64_t region_bytes, uint64_t region_block_offset, uint64_t byte_offset,
                            size_t window_bytes, pose_b200_sink_fn sink, void *sink_ctx,
                            const pose_b200_sched_t *sched, pose_b200_stats_t *stats)
@@ -198,5 +199,16 @@ out:
     pthread_mutex_destroy(&s.mu);
     pthread_cond_destroy(&s.cv);
     (void)label_ms;
+    return rc;
+}
+
+int pose_b200_label_stream(const pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
+                           uint64_t region_bytes, uint64_t region_block_offset, uint64_t byte_offset,
+                           size_t window_bytes, pose_b200_sink_fn sink, void *sink_ctx,
+                           const pose_b200_sched_t *sched, pose_b200_stats_t *stats)
+{
+    nvtxRangePushA("pose_b200: streamed labeling");
+    int rc = pose_b200_label_stream_impl(topo, session_seed, seed_len, region_bytes, region_block_offset, byte_offset, window_bytes, sink, sink_ctx, sched, stats);
+    nvtxRangePop();
     return rc;
 }

@@ -18,6 +18,7 @@
 #include "pose_b200.h"
 #include "topo_internal.h"
 
+#include <nvtx3/nvToolsExt.h>
 #include <cuda_runtime_api.h>
 #include <pthread.h>
 #include <stdio.h>
@@ -117,7 +118,7 @@ static int recompute(const pose_hbm_topo_t *topo, const pb_topo_internal_t *ti, 
     return rc;
 }
 
-int pose_b200_challenge_blocks(const pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
+static int pose_b200_challenge_blocks_impl(const pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
                                const uint64_t *blocks, size_t n, uint8_t *out,
                                const pose_b200_sched_t *sched, pose_b200_stats_t *stats)
 {
@@ -218,6 +219,16 @@ out:
     return rc;
 }
 
+int pose_b200_challenge_blocks(const pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
+                               const uint64_t *blocks, size_t n, uint8_t *out,
+                               const pose_b200_sched_t *sched, pose_b200_stats_t *stats)
+{
+    nvtxRangePushA("pose_b200: challenge blocks");
+    int rc = pose_b200_challenge_blocks_impl(topo, session_seed, seed_len, blocks, n, out, sched, stats);
+    nvtxRangePop();
+    return rc;
+}
+
 /* ── sampled verify ──────────────────────────────────────────────────────── */
 
 typedef struct {
@@ -241,7 +252,7 @@ static void *recompute_thread(void *arg)
     return NULL;
 }
 
-int pose_b200_verify_sampled(const pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
+static int pose_b200_verify_sampled_impl(const pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
                              uint64_t wipe_len, uint64_t samples, pose_b200_read_fn read, void *read_ctx,
                              uint64_t *checked_out, uint64_t *mism_out, uint64_t *first_bad,
                              const pose_b200_sched_t *sched, pose_b200_stats_t *stats)
@@ -361,5 +372,16 @@ out:
         stats->kernel_ms = acc.kernel_ms;
     }
     if (prev >= 0 && prev != ti.device) cudaSetDevice(prev);
+    return rc;
+}
+
+int pose_b200_verify_sampled(const pose_hbm_topo_t *topo, const uint8_t *session_seed, size_t seed_len,
+                             uint64_t wipe_len, uint64_t samples, pose_b200_read_fn read, void *read_ctx,
+                             uint64_t *checked_out, uint64_t *mism_out, uint64_t *first_bad,
+                             const pose_b200_sched_t *sched, pose_b200_stats_t *stats)
+{
+    nvtxRangePushA("pose_b200: sampled verify");
+    int rc = pose_b200_verify_sampled_impl(topo, session_seed, seed_len, wipe_len, samples, read, read_ctx, checked_out, mism_out, first_bad, sched, stats);
+    nvtxRangePop();
     return rc;
 }
