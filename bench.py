@@ -291,7 +291,7 @@ def run_served(pkg, torch, requests: int = 300, alone: bool = False) -> dict:
         o += sz
     keys = {r["session"]: r["key"] for r in trace}
     lat = [0.0] * len(trace)
-    with pkg.Server(scratch_bytes=32 << 30, max_waves=8) as srv:
+    with pkg.Server(scratch_bytes=32 << 30) as srv:  # the library's default wave count
         sid = {s: srv.session(k) for s, k in keys.items()}
         tickets = [None] * len(trace)
         t0 = time.perf_counter()

@@ -368,7 +368,11 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
     pose_b200_server_t *s = (pose_b200_server_t *)calloc(1, sizeof(*s));
     if (!s) return NULL;
     cudaGetDevice(&s->device);
-    s->max_waves = max_waves ? (max_waves < PB_SERVER_MAX_WAVES ? max_waves : PB_SERVER_MAX_WAVES) : 4;
+    /* 3 by default: on a 120-request Poisson trace (200 requests/s, chunk_blocks
+     * 2^10..2^18) 2-3 concurrent waves served 319-342 MiB/s, 4 waves 280-323,
+     * 8 waves 278 and 16 waves 214, at equal or better p50/p99: fewer slots
+     * let arrivals gather into larger, better-packed waves */
+    s->max_waves = max_waves ? (max_waves < PB_SERVER_MAX_WAVES ? max_waves : PB_SERVER_MAX_WAVES) : 3;
     pthread_mutex_init(&s->mu, NULL);
     pthread_cond_init(&s->cv, NULL);
     if (scratch_bytes == 0) {
