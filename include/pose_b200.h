@@ -275,13 +275,31 @@ int pose_b200_verify_sampled(const pose_hbm_topo_t *topo, const uint8_t *session
  * The first call on a device looks up the arrays' device addresses
  * (cudaGetSymbolAddress); make that first call before any stream capture.
  * All calls share the same arrays: the work counter is cleared by each launch
- * and the scratch and seed table are zeroed before the call returns, but
+ * and the scratch, the seed table and the session seed copy are zeroed before
+ * the call returns (when it fails too), but
  * calls whose device work overlaps (from several host threads, or on several
  * topologies of one device at once) race on them and must be serialised by
  * the caller. */
 int pose_b200_topo_label_noalloc(const pose_hbm_topo_t *topo, const uint8_t *session_seed,
                                  size_t seed_len, void *hbm_dev_ptr, size_t hbm_len,
                                  uint64_t region_block_offset);
+
+/* Workspace audit (no reference counterpart).  *nonzero_bytes = the nonzero
+ * bytes left in the device memory that labeling calls on this topology use
+ * besides the caller's buffer: the scratch labels, the chunk-seed table and
+ * the session seed copy, plus, on the topology's device, the arrays of
+ * pose_b200_topo_label_noalloc.  Every labeling call and every autotuner
+ * trial zeroes them before it returns, whether it succeeded or not, so
+ * between calls this is 0: no label, chunk seed or session key of a past
+ * call stays on the device.  Synchronous; must not overlap a labeling call
+ * on the same topology.  Returns 0 on success, -1 on error. */
+int pose_b200_topo_residue(const pose_hbm_topo_t *topo, uint64_t *nonzero_bytes);
+
+/* The counting of the workspace audit on any device buffer of the current
+ * device: *nonzero_bytes = the nonzero bytes of dev_ptr[0, bytes).  dev_ptr
+ * must be 16-byte aligned.  Synchronous.  Returns 0 on success, -1 on
+ * error. */
+int pose_b200_count_nonzero(const void *dev_ptr, size_t bytes, uint64_t *nonzero_bytes);
 
 /* Last error message of the calling thread ("" when none). */
 const char *pose_b200_last_error(void);

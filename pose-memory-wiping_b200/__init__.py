@@ -113,6 +113,10 @@ def _declare(L: C.CDLL) -> None:
     L.pose_b200_topo_label_noalloc.argtypes = [C.c_void_p, _u8p, C.c_size_t, C.c_void_p, C.c_size_t,
                                                C.c_uint64]
     L.pose_b200_topo_label_noalloc.restype = C.c_int
+    L.pose_b200_topo_residue.argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
+    L.pose_b200_topo_residue.restype = C.c_int
+    L.pose_b200_count_nonzero.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64)]
+    L.pose_b200_count_nonzero.restype = C.c_int
     L.pose_b200_batch_create.argtypes = [C.POINTER(Request), C.c_size_t, C.POINTER(Sched)]
     L.pose_b200_batch_create.restype = C.c_void_p
     L.pose_b200_batch_autotune.argtypes = [C.POINTER(Request), C.c_size_t, C.POINTER(Sched), C.c_uint32,
@@ -172,6 +176,15 @@ def _bytes_arg(b: bytes | None):
     if b is None:
         return None
     return C.cast(C.create_string_buffer(bytes(b), max(1, len(b))), _u8p)
+
+
+def count_nonzero(dev_ptr: int, nbytes: int) -> int:
+    """pose_b200_count_nonzero: nonzero bytes of a 16-byte aligned device
+    buffer of the current device."""
+    n = C.c_uint64(0)
+    if load().pose_b200_count_nonzero(C.c_void_p(dev_ptr), nbytes, C.byref(n)) != 0:
+        raise RuntimeError(last_error())
+    return n.value
 
 
 def last_error() -> str:
@@ -236,6 +249,14 @@ class Topology:
         call (for callers that cannot allocate while labeling)."""
         return load().pose_b200_topo_label_noalloc(self.handle, _bytes_arg(seed), len(seed),
                                                    C.c_void_p(dev_ptr), nbytes, region_block_offset)
+
+    def residue(self) -> int:
+        """pose_b200_topo_residue: nonzero bytes left in the device workspace
+        of this topology's labeling calls (0 between calls)."""
+        n = C.c_uint64(0)
+        if load().pose_b200_topo_residue(self.handle, C.byref(n)) != 0:
+            raise RuntimeError(last_error())
+        return n.value
 
     def label_stream(self, seed: bytes, region_bytes: int, sink, region_block_offset: int = 0,
                      byte_offset: int = 0, window_bytes: int = 1 << 30, sched: Sched | None = None):

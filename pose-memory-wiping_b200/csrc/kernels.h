@@ -148,6 +148,10 @@ int pb_dev_label_ws_occupancy(uint32_t cta_threads, uint32_t smem_bytes, int *bl
 int pb_dev_compare_blocks(const void *a, const void *b, uint64_t nblocks, uint64_t blocks_per_group,
                           unsigned long long *first_bad, uint32_t grid, cudaStream_t stream);
 int pb_dev_gather_labels(const void *work, const uint64_t *src, uint32_t n, void *out, cudaStream_t stream);
+/* *d_count += the nonzero bytes of buf[0, bytes) (buf 16-byte aligned), with
+ * at most `grid` CTAs of 256 threads. */
+int pb_dev_count_nonzero(const void *buf, uint64_t bytes, unsigned long long *d_count, uint32_t grid,
+                         cudaStream_t stream);
 
 int pb_dev_set_keys(const uint32_t ksrc[8], const uint32_t kint[8], const uint32_t kseed[8]);
 int pb_dev_cv0_table(const void *recs, uint32_t S, uint32_t copies, void *cv0, cudaStream_t stream);

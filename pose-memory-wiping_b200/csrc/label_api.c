@@ -13,8 +13,9 @@
  *   - one persistent launch covers up to PB_MAX_CHUNKS_PER_LAUNCH chunks;
  *     its schedule (team warps T, units per team G, resident teams) comes
  *     from a throughput model over the topology's level widths;
- *   - the scratch pool is kept on the topology across calls (grown on
- *     demand) and zeroed at the end of every call and before it is freed.
+ *   - the workspace (scratch pool, chunk seeds, session seed copy) is kept
+ *     on the topology across calls (grown on demand) and zeroed at the end
+ *     of every call, failed calls included, and before it is freed.
  */
 #include "b3_host.h"
 #include "dev_alloc.h"
@@ -339,20 +340,25 @@ static int grow(void **p, uint64_t *have, uint64_t need, size_t elem)
     return 0;
 }
 
+/* Zero the whole workspace (scratch labels, chunk seeds, the session seed),
+ * best effort: after a failed call the context may refuse the memsets, and
+ * then there is nothing more a host can do. */
+static void wipe_workspace(pose_hbm_topo_t *t)
+{
+    if (t->d_scratch) cudaMemsetAsync(t->d_scratch, 0, t->scratch_alloc, t->stream);
+    if (t->d_seeds) cudaMemsetAsync(t->d_seeds, 0, t->seeds_alloc * 32, t->stream);
+    if (t->d_sess) cudaMemsetAsync(t->d_sess, 0, t->sess_alloc, t->stream);
+    cudaStreamSynchronize(t->stream);
+    cudaGetLastError();
+}
+
 static void free_workspace(pose_hbm_topo_t *t)
 {
-    if (t->d_scratch) {
-        cudaMemsetAsync(t->d_scratch, 0, t->scratch_alloc, t->stream);
-        cudaStreamSynchronize(t->stream);
-        cudaFree(t->d_scratch);
-    }
+    wipe_workspace(t);
+    cudaFree(t->d_scratch);
     t->d_scratch = NULL;
     t->scratch_alloc = 0;
-    if (t->d_seeds) {
-        cudaMemsetAsync(t->d_seeds, 0, t->seeds_alloc * 32, t->stream);
-        cudaStreamSynchronize(t->stream);
-        cudaFree(t->d_seeds);
-    }
+    cudaFree(t->d_seeds);
     t->d_seeds = NULL;
     t->seeds_alloc = 0;
     cudaFree(t->d_sess);
@@ -823,10 +829,12 @@ static int topo_label_core_impl(const pose_hbm_topo_t *ct, const uint8_t *sessio
             if (cudaEventElapsedTime(&ms, t->ev[1], t->ev[2]) != cudaSuccess) { cudaGetLastError(); ms = 0; }
             kms += ms;
         }
-        /* scratch and seeds never outlive the call (the reference zeroes its
-         * scratch before freeing it, label_gpu_warp.cu:236-238) */
+        /* scratch labels, chunk seeds and the session seed never outlive the
+         * call (the reference zeroes its scratch before freeing it,
+         * label_gpu_warp.cu:236-238) */
         CK(cudaMemsetAsync(t->d_scratch, 0, plan.scratch_bytes, t->stream), "scratch zero");
         CK(cudaMemsetAsync(t->d_seeds, 0, per_launch * 32, t->stream), "seed zero");
+        if (dev_seeds && seed_len) CK(cudaMemsetAsync(t->d_sess, 0, seed_len, t->stream), "seed zero");
         CK(cudaEventRecord(t->ev[3], t->stream), "event");
         CK(cudaStreamSynchronize(t->stream), "label");
         float tms = 0;
@@ -859,6 +867,8 @@ out:
     if (rc != 0) {
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) fprintf(stderr, "pose_graph_hbm_topo_label: CUDA error: %s\n", cudaGetErrorString(e));
+        /* a call that stopped part way clears whatever it got to write */
+        wipe_workspace(t);
     }
     if (prev >= 0 && prev != t->device) cudaSetDevice(prev);
     return rc;
@@ -1006,6 +1016,73 @@ fail:
     if (a) cudaEventDestroy(a);
     if (b) cudaEventDestroy(b);
     return rate;
+}
+
+/* ── workspace audit ─────────────────────────────────────────────────────── */
+
+int pb_noalloc_residue(int device, unsigned long long *d_count, uint32_t grid, cudaStream_t s);
+
+int pose_b200_topo_residue(const pose_hbm_topo_t *ct, uint64_t *nonzero_bytes)
+{
+    pose_hbm_topo_t *t = (pose_hbm_topo_t *)ct;
+    if (!t || !nonzero_bytes) { set_err("pose_b200_topo_residue: NULL argument"); return -1; }
+    *nonzero_bytes = 0;
+    int prev = -1, rc = -1;
+    cudaGetDevice(&prev);
+    if (prev != t->device && cudaSetDevice(t->device) != cudaSuccess) {
+        set_err("pose_b200_topo_residue: cannot select the topology's device");
+        return -1;
+    }
+    unsigned long long *d_count = NULL, h_count = 0;
+    const uint32_t grid = (uint32_t)(t->sms > 0 ? t->sms : 1) * 8u;
+    if (pb_dev_malloc((void **)&d_count, sizeof(*d_count)) != cudaSuccess) {
+        set_err("pose_b200_topo_residue: alloc failed");
+        goto out;
+    }
+    if (cudaMemsetAsync(d_count, 0, sizeof(*d_count), t->stream) != cudaSuccess ||
+        (t->d_scratch && pb_dev_count_nonzero(t->d_scratch, t->scratch_alloc, d_count, grid, t->stream) != 0) ||
+        (t->d_seeds && pb_dev_count_nonzero(t->d_seeds, t->seeds_alloc * 32, d_count, grid, t->stream) != 0) ||
+        (t->d_sess && pb_dev_count_nonzero(t->d_sess, t->sess_alloc, d_count, grid, t->stream) != 0) ||
+        pb_noalloc_residue(t->device, d_count, grid, t->stream) != 0 ||
+        cudaMemcpyAsync(&h_count, d_count, sizeof(h_count), cudaMemcpyDeviceToHost, t->stream) != cudaSuccess ||
+        cudaStreamSynchronize(t->stream) != cudaSuccess) {
+        set_err("pose_b200_topo_residue: CUDA error: %s", cudaGetErrorString(cudaGetLastError()));
+        goto out;
+    }
+    *nonzero_bytes = h_count;
+    rc = 0;
+out:
+    cudaFree(d_count);
+    if (prev >= 0 && prev != t->device) cudaSetDevice(prev);
+    return rc;
+}
+
+int pose_b200_count_nonzero(const void *dev_ptr, size_t bytes, uint64_t *nonzero_bytes)
+{
+    if (!nonzero_bytes || (bytes && !dev_ptr)) { set_err("pose_b200_count_nonzero: NULL argument"); return -1; }
+    *nonzero_bytes = 0;
+    if (bytes == 0) return 0;
+    if ((uintptr_t)dev_ptr & 15u) { set_err("pose_b200_count_nonzero: buffer not 16-byte aligned"); return -1; }
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 1;
+    unsigned long long *d_count = NULL, h_count = 0;
+    cudaStream_t st = NULL;
+    int rc = -1;
+    if (pb_dev_malloc((void **)&d_count, sizeof(*d_count)) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMemsetAsync(d_count, 0, sizeof(*d_count), st) != cudaSuccess ||
+        pb_dev_count_nonzero(dev_ptr, bytes, d_count, (uint32_t)sms * 8u, st) != 0 ||
+        cudaMemcpyAsync(&h_count, d_count, sizeof(h_count), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        set_err("pose_b200_count_nonzero: CUDA error: %s", cudaGetErrorString(cudaGetLastError()));
+    } else {
+        *nonzero_bytes = h_count;
+        rc = 0;
+    }
+    if (st) cudaStreamDestroy(st);
+    cudaFree(d_count);
+    return rc;
 }
 
 /* ── read-only access for the other translation units ────────────────────── */

@@ -47,7 +47,8 @@ struct pose_b200_batch {
     cudaGraph_t graph;
     cudaGraphExec_t exec;
     cudaEvent_t ev[6]; /* 0/3: replay start/end; 1/2: first launch's kernel; 4/5: fork/join */
-    void *d_blob;
+    void *d_blob; /* the requests' session seeds, back to back */
+    size_t blob_len;
     int nparts;
     batch_part_t part[2]; /* part[1]: the deep requests, when split */
     uint64_t scratch_bytes, nodes, super_chunks, units;
@@ -72,8 +73,10 @@ static void batch_free(pose_b200_batch_t *b)
         for (int i = 0; i < b->nparts; i++) {
             batch_part_t *q = &b->part[i];
             if (q->d_scratch) cudaMemsetAsync(q->d_scratch, 0, q->scratch_bytes, b->stream);
-            if (q->d_seeds) cudaMemsetAsync(q->d_seeds, 0, (size_t)q->super_chunks * 32, b->stream);
+            if (q->d_seeds) cudaMemsetAsync(q->d_seeds, 0, (size_t)q->njobs * 32, b->stream);
         }
+        /* the session seeds go with the batch */
+        if (b->d_blob) cudaMemsetAsync(b->d_blob, 0, b->blob_len ? b->blob_len : 1, b->stream);
         cudaStreamSynchronize(b->stream);
     }
     if (b->exec) cudaGraphExecDestroy(b->exec);
@@ -399,7 +402,9 @@ static int part_setup(pose_b200_batch_t *b, batch_part_t *q, const pb_plan_table
 }
 
 /* Capture one launch onto stream s: seeds, queue reset, labeling, scratch
- * zeroing (events e0/e1 around the labeling kernel when not NULL). */
+ * and chunk-seed zeroing (events e0/e1 around the labeling kernel when not
+ * NULL).  A replay leaves no label or chunk seed behind; the session seeds
+ * stay for the next replay and are zeroed when the batch is destroyed. */
 static int part_capture(const pose_b200_batch_t *b, const batch_part_t *q, cudaStream_t s, cudaEvent_t e0,
                         cudaEvent_t e1)
 {
@@ -422,6 +427,7 @@ static int part_capture(const pose_b200_batch_t *b, const batch_part_t *q, cudaS
     if (crc == 0) crc = pb_dev_label_multi(&p, q->grid, q->cta_threads, s);
     if (crc == 0 && e1) crc = cudaEventRecord(e1, s) == cudaSuccess ? 0 : -1;
     if (crc == 0) crc = cudaMemsetAsync(q->d_scratch, 0, q->scratch_bytes, s) == cudaSuccess ? 0 : -1;
+    if (crc == 0) crc = cudaMemsetAsync(q->d_seeds, 0, (size_t)q->njobs * 32, s) == cudaSuccess ? 0 : -1;
     return crc;
 }
 
@@ -492,6 +498,7 @@ no_split:
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
     if (nd && cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking) != cudaSuccess) goto fail;
     for (int i = 0; i < 6; i++) if (cudaEventCreate(&b->ev[i]) != cudaSuccess) goto fail;
+    b->blob_len = blob_len;
     if (pb_dev_malloc(&b->d_blob, blob_len ? blob_len : 1) != cudaSuccess) {
         fprintf(stderr, "pose_b200_batch_create: alloc: %s\n", cudaGetErrorString(cudaGetLastError()));
         goto fail;
@@ -571,6 +578,7 @@ no_split:
             goto fail;
         }
     }
+    if (blob) explicit_bzero(blob, blob_len);
     free(pr); free(pd); free(ps); free(deep); free(blob); pb_plan_free(&pl[0]); pb_plan_free(&pl[1]);
     return b;
 fail:
@@ -578,6 +586,7 @@ fail:
     b = NULL;
 fail_host:
     cudaGetLastError();
+    if (blob) explicit_bzero(blob, blob_len);
     free(pr); free(pd); free(ps); free(deep); free(blob); pb_plan_free(&pl[0]); pb_plan_free(&pl[1]);
     return NULL;
 }

@@ -149,15 +149,40 @@ extern "C" int pose_b200_topo_label_noalloc(const pose_hbm_topo_t *topo, const u
         p.one = 1;
         if (pb_dev_label(&p, plan.grid, plan.cta, s) != 0) goto cuda_fail;
     }
-    /* labels never outlive the call: clear the shared scratch and seed table */
+    /* labels and seeds never outlive the call: clear the shared scratch, the
+     * seed table and the session seed copy */
     if (cudaMemsetAsync(na.scratch, 0, plan.scratch_bytes, s) != cudaSuccess) goto cuda_fail;
     if (cudaMemsetAsync(na.seeds, 0, per_launch * 32, s) != cudaSuccess) goto cuda_fail;
+    if (seed_len && cudaMemsetAsync(na.session, 0, seed_len, s) != cudaSuccess) goto cuda_fail;
     if (cudaStreamSynchronize(s) != cudaSuccess) goto cuda_fail;
     rc = 0;
     goto out;
 cuda_fail:
     fprintf(stderr, "pose_b200_topo_label_noalloc: CUDA error: %s\n", cudaGetErrorString(cudaGetLastError()));
+    /* a call that stopped part way clears all three arrays, best effort */
+    cudaMemsetAsync(na.scratch, 0, PB_NOALLOC_SCRATCH_BYTES, s);
+    cudaMemsetAsync(na.seeds, 0, sizeof(g_na_seeds), s);
+    cudaMemsetAsync(na.session, 0, PB_NOALLOC_MAX_SEED, s);
+    cudaStreamSynchronize(s);
+    cudaGetLastError();
 out:
     if (prev >= 0 && prev != ti.device) cudaSetDevice(prev);
     return rc;
+}
+
+/* Count the nonzero bytes of this device's no-allocation workspace (scratch,
+ * seed table, session seed) into *d_count on stream s; nothing to count (0)
+ * when the entry point never ran on the device.  The device is current. */
+extern "C" int pb_noalloc_residue(int device, unsigned long long *d_count, uint32_t grid, cudaStream_t s)
+{
+    if (device < 0 || device >= PB_NOALLOC_MAX_DEVICES) return -1;
+    pthread_mutex_lock(&g_na_lock);
+    const na_addrs_t a = g_na_addrs[device];
+    pthread_mutex_unlock(&g_na_lock);
+    if (!a.ready) return 0;
+    if (pb_dev_count_nonzero(a.scratch, PB_NOALLOC_SCRATCH_BYTES, d_count, grid, s) != 0 ||
+        pb_dev_count_nonzero(a.seeds, sizeof(g_na_seeds), d_count, grid, s) != 0 ||
+        pb_dev_count_nonzero(a.session, PB_NOALLOC_MAX_SEED, d_count, grid, s) != 0)
+        return -1;
+    return 0;
 }

@@ -270,13 +270,20 @@ static int admit(pose_b200_server_t *s)
     p.unit_req = (const uint32_t *)(T + o_ureq);
     p.req_done = wv->d_done;
     if (ok) ok = pb_dev_label_multi(&p, g2, 32 * Tw * tpc, wv->stream) == 0;
-    /* the range is zeroed before the wave counts as done */
+    /* the scratch range and the chunk seeds are zeroed before the wave
+     * counts as done */
     if (ok) ok = cudaMemsetAsync(s->d_arena + off, 0, scratch, wv->stream) == cudaSuccess;
+    if (ok) ok = cudaMemsetAsync(T + o_seeds, 0, pl.njobs * 32, wv->stream) == cudaSuccess;
     if (ok) ok = cudaEventRecord(wv->done, wv->stream) == cudaSuccess;
     double t = now_ms();
     if (!ok) {
         fprintf(stderr, "pose_b200_server: wave launch failed: %s\n", cudaGetErrorString(cudaGetLastError()));
         cudaStreamSynchronize(wv->stream);
+        /* whatever the wave got to write goes, best effort */
+        cudaMemsetAsync(s->d_arena + off, 0, scratch, wv->stream);
+        cudaMemsetAsync(T + o_seeds, 0, pl.njobs * 32, wv->stream);
+        cudaStreamSynchronize(wv->stream);
+        cudaGetLastError();
         arena_give(s, off, scratch);
         for (size_t i = first; i < last; i++) { s->reqs[i].state = 3; s->reqs[i].t_done = t; }
     } else {

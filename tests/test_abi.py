@@ -69,3 +69,12 @@ def test_headers_compile_as_c11_and_cxx():
         r = subprocess.run([compiler, std, "-Wall", "-Werror", "-fsyntax-only", "-I", inc, "-x", lang, "-"],
                            input=src, text=True, capture_output=True)
         assert r.returncode == 0, r.stderr
+
+
+def test_workspace_audit_rejects_bad_arguments(pkg):
+    L = pkg.load()
+    n = C.c_uint64(7)
+    assert L.pose_b200_topo_residue(None, C.byref(n)) == -1
+    assert L.pose_b200_count_nonzero(None, 16, C.byref(n)) == -1
+    assert L.pose_b200_count_nonzero(C.c_void_p(0x1001), 16, C.byref(n)) == -1  # not 16-byte aligned
+    assert L.pose_b200_count_nonzero(None, 0, C.byref(n)) == 0 and n.value == 0  # nothing to count
