@@ -162,7 +162,7 @@ def cpu_reference(w: dict, steps: int, warmup: int, cores: int | None = None) ->
     """Time the reference's own CPU in-place labeler (oracle/_ref) on a
     bounded sample: one super-chunk per host thread per step."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from oracle import RefCPU  # test-infrastructure checker, CPU legs only
+    from oracle import RefCPU  # test infrastructure: the reference's CPU labeler, CPU legs only
     ref = RefCPU()
     cores = cores or os.cpu_count() or 1
     cb = w["chunk_blocks"]
@@ -472,7 +472,7 @@ def run_b200(args) -> None:
         try:
             cpu = cpu_reference(w, 1, 0)
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
-        except Exception as exc:  # the checker build may be absent
+        except Exception as exc:  # the oracle's reference build may be absent
             line["cpu_baseline"] = {"value": None, "unit": "MiB/s", "cores": os.cpu_count(), "kind": "reference",
                                     "sample": f"unavailable: {exc}"}
     topo.free()

@@ -1,6 +1,6 @@
 """TEST INFRASTRUCTURE ONLY: ctypes bindings for the CPU oracle.
 
-Two checkers live here, both used only by tests/, ``__graft_entry__.smoke()``
+Two oracles live here, both used only by tests/, ``__graft_entry__.smoke()``
 and the bench's CPU-baseline / reference legs, never by the product path:
 
 * ``Oracle`` — ``oracle/_build/liboracle.so``, the C restatement of the

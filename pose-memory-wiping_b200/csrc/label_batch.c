@@ -607,8 +607,8 @@ static int pose_b200_batch_run_impl(pose_b200_batch_t *b, pose_b200_stats_t *sta
     if (stats) {
         float k = 0, t = 0;
         if (cudaEventElapsedTime(&t, b->ev[0], b->ev[3]) != cudaSuccess) { cudaGetLastError(); t = 0; }
-        /* the kernel's own events are nodes of the graph; where the driver
-         * does not time them, or two launches overlap, report the replay */
+        /* the kernel's own events are nodes of the graph; where the CUDA
+         * driver does not time them, or two launches overlap, report the replay */
         if (b->nparts > 1 || cudaEventElapsedTime(&k, b->ev[1], b->ev[2]) != cudaSuccess || k <= 0) {
             cudaGetLastError();
             k = t;
