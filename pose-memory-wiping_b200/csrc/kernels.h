@@ -141,6 +141,32 @@ int pb_dev_label_ws(const pb_pipe_params_t *params, uint32_t grid, uint32_t cta_
                     uint32_t smem_bytes, cudaStream_t stream);
 int pb_dev_label_ws_occupancy(uint32_t cta_threads, uint32_t smem_bytes, int *blocks_per_sm);
 
+/* Multi-unit depth kernel (label_ws.cu): k_label_ws with up to 2^g_log2
+ * units of one topology per CTA in lockstep.  Batch b is units
+ * [b << g_log2, min(nunits, (b + 1) << g_log2)) of `units`; unit k's global
+ * label pool is scratch + (cta * G + k % G) * unit_scratch_bytes.  The
+ * topology's pipelined records are built for a pool of topo.csm slots per
+ * unit, and shared memory holds G such pools (pb_wsg_smem_bytes). */
+typedef struct {
+    pb_topo_view2_t topo;
+    const pb_munit_t *units;
+    const uint32_t *seeds;       /* 8 words per seed index (pb_munit_t.seed) */
+    uint8_t *scratch;
+    uint64_t unit_scratch_bytes; /* topo.gpool * 32 */
+    uint32_t nunits;
+    uint32_t g_log2;             /* 0, 1 or 2 */
+    uint32_t team_warps;         /* hashing warps: 7 or 15 */
+    uint32_t nbatches;           /* ceil(nunits / G) */
+    unsigned int *queue;         /* zeroed work counter */
+} pb_wsg_params_t;
+
+uint32_t pb_wsg_smem_bytes(uint32_t csm, uint32_t g_log2, uint32_t team_warps);
+int pb_dev_label_wsg(const pb_wsg_params_t *params, uint32_t grid, uint32_t cta_threads, uint32_t smem_bytes,
+                     cudaStream_t stream);
+/* Raise k_label_wsg's dynamic shared memory limit to the most a CTA can
+ * have and report it; before any launch or stream capture of it. */
+int pb_dev_label_wsg_prepare(uint32_t *max_smem_bytes);
+
 /* Verifier helpers (label_verify.cu).  Compare nblocks 32-byte blocks of a
  * and b, grouped blocks_per_group to a group: first_bad[g] = min over
  * mismatching blocks of their index within group g (initialise it to all

@@ -95,6 +95,10 @@ struct pose_hbm_topo {
     size_t sess_alloc;
     unsigned int *d_queue;
     int occ256, occ512, sms;
+    /* pipelined records for a PB_CSM_MULTI-slot shared pool per unit (the
+     * multi-unit depth kernel's), built on first use */
+    void *d_recs2s;
+    pb_topo_view2_t view2s;
     /* schedule chosen by pose_b200_topo_autotune for calls of tuned_units chunk copies */
     int tuned_ok;
     uint64_t tuned_units;
@@ -135,6 +139,7 @@ typedef struct {
 } plan_t;
 
 #define PB_CSM_LATENCY 2048u /* shared-memory label slots per copy in the pipelined records */
+#define PB_CSM_MULTI 512u    /* the same for the multi-unit depth kernel (four pools per CTA) */
 
 static uint32_t pipe_smem_bytes(const pose_hbm_topo_t *t, uint32_t T, uint32_t G)
 {
@@ -377,6 +382,7 @@ void pose_graph_hbm_topo_free(pose_hbm_topo_t *t)
     if (t->stream) free_workspace(t);
     cudaFree(t->d_recs);
     cudaFree(t->d_recs2);
+    cudaFree(t->d_recs2s);
     cudaFree(t->d_cv0);
     cudaFree(t->d_orank);
     cudaFree(t->d_lstart);
@@ -1099,6 +1105,40 @@ int pb_topo_internal(const pose_hbm_topo_t *t, pb_topo_internal_t *out)
     out->view = t->view;
     out->stream = t->stream;
     out->sms = t->sms;
+    return 0;
+}
+
+int pb_topo_view2_small(const pose_hbm_topo_t *ct, pb_topo_view2_t *out)
+{
+    pose_hbm_topo_t *t = (pose_hbm_topo_t *)ct; /* the record set is built once and kept */
+    if (!t || !out || !t->d_cv0 || !t->d_recs2) return -1;
+    if (!t->d_recs2s) {
+        pb_topo_host_t h;
+        if (pb_topo_host_build_ex(t->cb, PB_CSM_MULTI, &h) != 0) return -1;
+        /* the same levels and node order as the default records; only the
+         * pool slots differ */
+        int ok = h.recs2 && h.S == t->S && h.L == t->L;
+        int prev = -1;
+        cudaGetDevice(&prev);
+        if (ok && prev != t->device) ok = cudaSetDevice(t->device) == cudaSuccess;
+        if (ok) ok = pb_dev_malloc(&t->d_recs2s, (size_t)h.S * 32) == cudaSuccess;
+        if (ok) ok = cudaMemcpy(t->d_recs2s, h.recs2, (size_t)h.S * 32, cudaMemcpyHostToDevice) == cudaSuccess;
+        if (ok) {
+            t->view2s = t->view2;
+            t->view2s.recs2 = (const pb_u4 *)t->d_recs2s;
+            t->view2s.csm = h.csm;
+            t->view2s.gpool = h.gpool2;
+            t->dev_bytes += (uint64_t)h.S * 32;
+        } else {
+            cudaFree(t->d_recs2s);
+            t->d_recs2s = NULL;
+            cudaGetLastError();
+        }
+        if (prev >= 0 && prev != t->device) cudaSetDevice(prev);
+        pb_topo_host_free(&h);
+        if (!ok) return -1;
+    }
+    *out = t->view2s;
     return 0;
 }
 

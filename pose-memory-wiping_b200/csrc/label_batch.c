@@ -33,12 +33,17 @@
 #include <stdlib.h>
 #include <string.h>
 
-/* One launch of a batch: its tables, scratch and queue. */
+/* One launch of a batch: its tables, scratch and queue.  kind 0 runs the
+ * lockstep multi-topology kernel, kind 1 the multi-unit depth kernel (one
+ * topology; v2, glog and smem describe it). */
 typedef struct {
     void *d_topos, *d_batches, *d_units, *d_jobs, *d_seeds, *d_scratch, *d_queue;
     uint64_t scratch_bytes, nodes, super_chunks, units, nbatches, njobs;
     uint32_t teams, T, Gmax, fma, cv0, grid, cta_threads;
     uint64_t team_scratch;
+    int kind;
+    pb_topo_view2_t v2;
+    uint32_t glog, smem;
 } batch_part_t;
 
 struct pose_b200_batch {
@@ -401,6 +406,56 @@ static int part_setup(pose_b200_batch_t *b, batch_part_t *q, const pb_plan_table
     return 0;
 }
 
+/* The deep part on the multi-unit depth kernel: every unit of pl (one
+ * topology, records v2), 2^glog units per CTA, at most one CTA per SM
+ * (`sms` CTAs), 15 hashing warps.  Returns 0, or -1 (message on stderr). */
+static int part_setup_wsg(pose_b200_batch_t *b, batch_part_t *q, const pb_plan_tables_t *pl,
+                          const pb_topo_view2_t *v2, uint32_t glog, uint32_t sms, uint32_t smem)
+{
+    const uint32_t G = 1u << glog, NC = 15;
+    q->kind = 1;
+    q->v2 = *v2;
+    q->glog = glog;
+    q->T = NC;
+    q->units = pl->nunits;
+    q->njobs = pl->njobs;
+    q->super_chunks = pl->njobs;
+    q->nodes = pl->nodes;
+    q->Gmax = G;
+    q->cv0 = 1;
+    q->fma = 0;
+    q->nbatches = (pl->nunits + G - 1) / G;
+    q->grid = (uint32_t)(q->nbatches < sms ? q->nbatches : sms);
+    q->teams = q->grid;
+    q->cta_threads = 32 * (NC + 1);
+    q->smem = smem;
+    q->team_scratch = (uint64_t)G * v2->gpool * 32;
+    q->scratch_bytes = (uint64_t)q->grid * q->team_scratch;
+    uint32_t max_smem = 0;
+    if (pb_dev_label_wsg_prepare(&max_smem) != 0 || pb_wsg_smem_bytes(v2->csm, glog, NC) > max_smem) {
+        fprintf(stderr, "pose_b200_batch_create: shared memory attribute: %s\n", cudaGetErrorString(cudaGetLastError()));
+        return -1;
+    }
+    if (q->smem > max_smem) q->smem = max_smem;
+    if (pb_dev_malloc(&q->d_units, pl->nunits * sizeof(pb_munit_t)) != cudaSuccess ||
+        pb_dev_malloc(&q->d_jobs, pl->njobs * sizeof(pb_seedjob_t)) != cudaSuccess ||
+        pb_dev_malloc(&q->d_seeds, pl->njobs * 32) != cudaSuccess ||
+        pb_dev_malloc(&q->d_scratch, q->scratch_bytes) != cudaSuccess ||
+        pb_dev_malloc(&q->d_queue, 64) != cudaSuccess) {
+        fprintf(stderr, "pose_b200_batch_create: alloc: %s\n", cudaGetErrorString(cudaGetLastError()));
+        return -1;
+    }
+    if (cudaMemcpyAsync(q->d_units, pl->units, pl->nunits * sizeof(pb_munit_t), cudaMemcpyHostToDevice,
+                        b->stream) != cudaSuccess ||
+        cudaMemcpyAsync(q->d_jobs, pl->jobs, pl->njobs * sizeof(pb_seedjob_t), cudaMemcpyHostToDevice,
+                        b->stream) != cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess) {
+        fprintf(stderr, "pose_b200_batch_create: upload: %s\n", cudaGetErrorString(cudaGetLastError()));
+        return -1;
+    }
+    return 0;
+}
+
 /* Capture one launch onto stream s: seeds, queue reset, labeling, scratch
  * and chunk-seed zeroing (events e0/e1 around the labeling kernel when not
  * NULL).  A replay leaves no label or chunk seed behind; the session seeds
@@ -424,7 +479,23 @@ static int part_capture(const pose_b200_batch_t *b, const batch_part_t *q, cudaS
     int crc = pb_dev_seed_jobs(q->d_jobs, (uint32_t)q->njobs, (const uint8_t *)b->d_blob, (uint32_t *)q->d_seeds, s);
     if (crc == 0) crc = cudaMemsetAsync(q->d_queue, 0, 64, s) == cudaSuccess ? 0 : -1;
     if (crc == 0 && e0) crc = cudaEventRecord(e0, s) == cudaSuccess ? 0 : -1;
-    if (crc == 0) crc = pb_dev_label_multi(&p, q->grid, q->cta_threads, s);
+    if (crc == 0 && q->kind == 1) {
+        pb_wsg_params_t w;
+        memset(&w, 0, sizeof(w));
+        w.topo = q->v2;
+        w.units = (const pb_munit_t *)q->d_units;
+        w.seeds = (const uint32_t *)q->d_seeds;
+        w.scratch = (uint8_t *)q->d_scratch;
+        w.unit_scratch_bytes = (uint64_t)q->v2.gpool * 32;
+        w.nunits = (uint32_t)q->units;
+        w.g_log2 = q->glog;
+        w.team_warps = q->T;
+        w.nbatches = (uint32_t)q->nbatches;
+        w.queue = (unsigned int *)q->d_queue;
+        crc = pb_dev_label_wsg(&w, q->grid, q->cta_threads, q->smem, s);
+    } else if (crc == 0) {
+        crc = pb_dev_label_multi(&p, q->grid, q->cta_threads, s);
+    }
     if (crc == 0 && e1) crc = cudaEventRecord(e1, s) == cudaSuccess ? 0 : -1;
     if (crc == 0) crc = cudaMemsetAsync(q->d_scratch, 0, q->scratch_bytes, s) == cudaSuccess ? 0 : -1;
     if (crc == 0) crc = cudaMemsetAsync(q->d_seeds, 0, (size_t)q->njobs * 32, s) == cudaSuccess ? 0 : -1;
@@ -516,18 +587,41 @@ no_split:
         if (nd) {
             uint64_t dunits = 0;
             uint32_t sms = 148;
+            int one_topo = 1;
             for (size_t i = 0; i < nd; i++) {
                 pb_topo_internal_t x;
                 if (pb_topo_internal(pd[i].topo, &x) != 0) goto fail;
                 dunits += (uint64_t)(pd[i].len / x.super_bytes) * x.copies;
                 sms = (uint32_t)x.sms;
+                if (pd[i].topo != pd[0].topo) one_topo = 0;
             }
-            uint32_t g = 1;
-            while (g < 4 && 2 * (dunits + g - 1) / g > (uint64_t)sms * occ) g *= 2;
-            if (pb_plan_requests(pd, nd, 8, g, 0.9999, &pl[1]) != 0 || pl[1].nunits == 0) goto fail;
-            deep_ctas = pl[1].nbatches;
-            if (deep_ctas * 2 > (uint64_t)pl[1].sms * occ) deep_ctas = (uint64_t)pl[1].sms * occ / 2;
-            if (part_setup(b, &b->part[1], &pl[1], 8, deep_ctas, budget, NULL) != 0) goto fail;
+            /* one topology: the multi-unit depth kernel, with the fewest
+             * units per CTA (1, 2 or 4) that fit one CTA per SM */
+            pb_topo_view2_t v2;
+            uint32_t glog = 0;
+            while (glog < 2 && ((dunits + (1u << glog) - 1) >> glog) > sms) glog++;
+            const char *ek = getenv("POSE_B200_DEEP_KERNEL");
+            const char *eg = getenv("POSE_B200_DEEP_UNITS");
+            if (eg && (eg[0] == '1' || eg[0] == '2' || eg[0] == '4') && !eg[1]) glog = eg[0] == '1' ? 0 : eg[0] == '2' ? 1 : 2;
+            int wsg = !(ek && ek[0] == '0') && one_topo && pb_topo_view2_small(pd[0].topo, &v2) == 0;
+            if (wsg) {
+                const uint64_t grid = ((dunits + (1u << glog) - 1) >> glog) < sms ? ((dunits + (1u << glog) - 1) >> glog) : sms;
+                wsg = grid * ((uint64_t)v2.gpool * 32 << glog) <= budget;
+            }
+            if (wsg) {
+                const char *ex = getenv("POSE_B200_DEEP_EXCLUSIVE");
+                uint32_t smem = pb_wsg_smem_bytes(v2.csm, glog, 15);
+                if (ex && ex[0] == '1') smem = 0xFFFFFFFFu; /* the most a CTA can have: no other CTA fits beside it */
+                if (pb_plan_requests(pd, nd, 8, 1, 0.9999, &pl[1]) != 0 || pl[1].nunits == 0) goto fail;
+                if (part_setup_wsg(b, &b->part[1], &pl[1], &v2, glog, sms, smem) != 0) goto fail;
+            } else {
+                uint32_t g = 1;
+                while (g < 4 && 2 * (dunits + g - 1) / g > (uint64_t)sms * occ) g *= 2;
+                if (pb_plan_requests(pd, nd, 8, g, 0.9999, &pl[1]) != 0 || pl[1].nunits == 0) goto fail;
+                deep_ctas = pl[1].nbatches;
+                if (deep_ctas * 2 > (uint64_t)pl[1].sms * occ) deep_ctas = (uint64_t)pl[1].sms * occ / 2;
+                if (part_setup(b, &b->part[1], &pl[1], 8, deep_ctas, budget, NULL) != 0) goto fail;
+            }
             budget = budget > b->part[1].scratch_bytes ? budget - b->part[1].scratch_bytes : 0;
         }
         const uint32_t gcap = sched && sched->units_per_team ? sched->units_per_team : 32;

@@ -92,8 +92,8 @@ __device__ __forceinline__ void store_label(const Unit &un, const Smem &sm, uint
     }
 }
 
-__device__ __forceinline__ void hash_node(const pb_pipe_params_t &p, const Unit &un, uint32_t (&cv)[8],
-                                          const uint32_t (&m)[16])
+template <class P>
+__device__ __forceinline__ void hash_node(const P &p, const Unit &un, uint32_t (&cv)[8], const uint32_t (&m)[16])
 {
     compress(cv, m, 64, kFlagsBlock1);
     uint32_t m2[16];
@@ -112,8 +112,8 @@ __device__ __forceinline__ void load_prev(const Unit &un, const Smem &sm, uint32
 }
 
 /* An item with everything loaded on the spot (wide levels). */
-__device__ __forceinline__ void direct_item(const pb_pipe_params_t &p, const Unit &un, const Smem &sm,
-                                            uint32_t pos)
+template <class P>
+__device__ __forceinline__ void direct_item(const P &p, const Unit &un, const Smem &sm, uint32_t pos)
 {
     const uint4 *rp = p.topo.recs2 + 2 * (size_t)pos;
     const uint4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
@@ -135,7 +135,8 @@ __device__ __forceinline__ void direct_item(const pb_pipe_params_t &p, const Uni
 }
 
 /* Producer: records of `lv` (when < L) into ring stage lv % 3, and its header. */
-__device__ __forceinline__ void stage_records(const pb_pipe_params_t &p, const Smem &sm, uint32_t lv, uint32_t lane)
+template <class P, class S>
+__device__ __forceinline__ void stage_records(const P &p, const S &sm, uint32_t lv, uint32_t lane)
 {
     const pb_topo_view2_t &tp = p.topo;
     if (lv >= tp.L) return;
@@ -268,6 +269,171 @@ __global__ void __launch_bounds__(PB_CTA_THREADS, 1) k_label_ws(const __grid_con
     }
 }
 
+namespace {
+
+/* Shared-memory layout of the multi-unit kernel (uint4 units):
+ *   pool  [G][csm][2]   next-level labels, one pool per unit
+ *   rec   [3][slots][2] records of up to `slots` nodes per level (shared by the units)
+ *   dat   [2][items][6] cv0 (2), predecessor 0 (2), predecessor 1 (2) per item
+ *   hdr   [3]           (level start, width) of each ring stage
+ * items = hashing threads, slots = items / G; item i is node i >> g_log2 of
+ * the batch's unit i & (G - 1). */
+struct SmemG {
+    uint4 *pool, *rec, *dat, *hdr;
+    uint32_t slots, items;
+    __device__ __forceinline__ uint4 *r(uint32_t st, uint32_t j) const { return rec + ((size_t)st * slots + j) * 2; }
+    __device__ __forceinline__ uint4 *d(uint32_t st, uint32_t i) const { return dat + ((size_t)st * items + i) * 6; }
+};
+
+/* Producer: block-0 values and older predecessors of level `lv` into data
+ * stage lv & 1, for every item of the level's staged nodes whose unit is in
+ * the batch (cnt units; s_copy = their copies). */
+__device__ __forceinline__ void stage_data_g(const pb_wsg_params_t &p, const SmemG &sm, const uint32_t *s_copy,
+                                             uint32_t cnt, uint32_t lv, uint32_t ls, uint32_t w, uint32_t lane)
+{
+    if (lv >= p.topo.L) return;
+    const uint32_t G = 1u << p.g_log2;
+    const uint32_t ns = w < sm.slots ? w : sm.slots;
+    const uint32_t rs = lv % 3, ds = lv & 1;
+    for (uint32_t i = lane; i < (ns << p.g_log2); i += 32) {
+        const uint32_t j = i >> p.g_log2, u = i & (G - 1);
+        if (u >= cnt) continue;
+        const uint4 r0 = *sm.r(rs, j);
+        uint4 *d = sm.d(ds, i);
+        const uint4 *c = p.topo.cv0 + ((size_t)s_copy[u] * p.topo.S + ls + j) * 2;
+        cp_async16(d, c);
+        cp_async16(d + 1, c + 1);
+        const uint4 *gs =
+            reinterpret_cast<const uint4 *>(p.scratch + ((uint64_t)blockIdx.x * G + u) * p.unit_scratch_bytes);
+        const uint32_t np = (r0.x >> PB_REC_NP_SHIFT) & 3u;
+        if (np >= 1 && !(r0.y & PB_REF_PREV)) {
+            const uint4 *s = gs + (size_t)(r0.y & PB_REF_SLOT_MASK) * 2;
+            cp_async16(d + 2, s);
+            cp_async16(d + 3, s + 1);
+        }
+        if (np >= 2 && !(r0.z & PB_REF_PREV)) {
+            const uint4 *s = gs + (size_t)(r0.z & PB_REF_SLOT_MASK) * 2;
+            cp_async16(d + 4, s);
+            cp_async16(d + 5, s + 1);
+        }
+    }
+}
+
+} /* namespace */
+
+/* k_label_ws with G units of one topology per CTA.  The producer warp stages
+ * each level's records once for all units and the block-0 values and older
+ * predecessors of every (node, unit) item; hashing thread c works item c
+ * (node c >> g_log2 of unit c & (G - 1)) and, on levels wider than the
+ * staged slots, that unit's further nodes with direct loads.  One CTA
+ * barrier ends a level, as in k_label_ws; there are no spin-waits. */
+__global__ void __launch_bounds__(PB_CTA_THREADS, 1) k_label_wsg(const __grid_constant__ pb_wsg_params_t p)
+{
+    extern __shared__ uint4 smem[];
+    __shared__ uint32_t s_batch, s_cnt;
+    __shared__ uint32_t s_copy[4];
+    const pb_topo_view2_t &tp = p.topo;
+    const uint32_t NC = p.team_warps;
+    const uint32_t nthr = NC * 32;
+    const uint32_t G = 1u << p.g_log2;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool producer = warp == NC;
+    const uint32_t c = threadIdx.x;
+    const uint32_t u = c & (G - 1), j0 = c >> p.g_log2;
+    SmemG sg;
+    sg.items = nthr;
+    sg.slots = nthr >> p.g_log2;
+    sg.pool = smem;
+    sg.rec = sg.pool + (size_t)G * tp.csm * 2;
+    sg.dat = sg.rec + (size_t)3 * sg.slots * 2;
+    sg.hdr = sg.dat + (size_t)2 * nthr * 6;
+    Smem su; /* this thread's unit pool, for load_prev / store_label / direct_item */
+    su.pool = sg.pool + (size_t)u * tp.csm * 2;
+    su.rec = su.dat = su.hdr = nullptr;
+    su.slots = 0;
+    Unit un;
+    un.gscr = reinterpret_cast<uint4 *>(p.scratch + ((uint64_t)blockIdx.x * G + u) * p.unit_scratch_bytes);
+
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const uint32_t b = atomicAdd(p.queue, 1u);
+            s_batch = b;
+            s_cnt = 0;
+            if (b < p.nbatches) {
+                const uint32_t left = p.nunits - (b << p.g_log2);
+                s_cnt = left < G ? left : G;
+                for (uint32_t k = 0; k < s_cnt; k++) s_copy[k] = p.units[(b << p.g_log2) + k].copy;
+            }
+        }
+        __syncthreads();
+        const uint32_t batch = s_batch, cnt = s_cnt;
+        __syncthreads();
+        if (batch >= p.nbatches) break;
+        const bool act = !producer && u < cnt;
+        if (act) {
+            const pb_munit_t mu = p.units[(batch << p.g_log2) + u];
+            un.copy = mu.copy;
+            un.rank_base = mu.copy ? tp.half_w : 0u;
+            un.rank_lim = mu.copy ? tp.retained : tp.half_w;
+            un.out = reinterpret_cast<uint8_t *>(mu.out);
+            un.cv0 = tp.cv0 + (uint64_t)mu.copy * tp.S * 2;
+#pragma unroll
+            for (int i = 0; i < 8; i++) un.seed[i] = p.seeds[8 * (size_t)mu.seed + i];
+        }
+
+        /* prologue: records of levels 0 and 1, then level 0's data */
+        if (producer) {
+            stage_records(p, sg, 0, lane);
+            stage_records(p, sg, 1, lane);
+            cp_async_commit();
+            cp_async_wait_all();
+            __syncwarp();
+            const uint32_t ls0 = __ldg(tp.lstart), w0 = __ldg(tp.lstart + 1) - ls0;
+            stage_data_g(p, sg, s_copy, cnt, 0, ls0, w0, lane);
+            cp_async_commit();
+            cp_async_wait_all();
+        }
+        __syncthreads();
+
+        for (uint32_t l = 0; l < tp.L; l++) {
+            if (producer) {
+                stage_records(p, sg, l + 2, lane);
+                if (l + 1 < tp.L) {
+                    const uint4 h = sg.hdr[(l + 1) % 3];
+                    stage_data_g(p, sg, s_copy, cnt, l + 1, h.x, h.y, lane);
+                }
+                cp_async_commit();
+                cp_async_wait_all();
+            } else if (act) {
+                const uint4 h = sg.hdr[l % 3];
+                const uint32_t ls = h.x, w = h.y;
+                const uint32_t ns = w < sg.slots ? w : sg.slots;
+                if (j0 < ns) {
+                    const uint4 r0 = *sg.r(l % 3, j0), r1 = *(sg.r(l % 3, j0) + 1);
+                    const uint4 *d = sg.d(l & 1, c);
+                    const uint32_t np = (r0.x >> PB_REC_NP_SHIFT) & 3u;
+                    uint32_t m[16], cv[8];
+#pragma unroll
+                    for (int i = 0; i < 16; i++) m[i] = 0;
+                    if (np >= 1) {
+                        if (r0.y & PB_REF_PREV) load_prev(un, su, r0.y, m);
+                        else put8(m, d[2], d[3]);
+                    }
+                    if (np >= 2) {
+                        if (r0.z & PB_REF_PREV) load_prev(un, su, r0.z, m + 8);
+                        else put8(m + 8, d[4], d[5]);
+                    }
+                    put8(cv, d[0], d[1]);
+                    hash_node(p, un, cv, m);
+                    store_label(un, su, r0, r1, cv);
+                }
+                for (uint32_t j = j0 + sg.slots; j < w; j += sg.slots) direct_item(p, un, su, ls + j);
+            }
+            __syncthreads();
+        }
+    }
+}
+
 } /* namespace pb */
 
 extern "C" int pb_dev_label_ws(const pb_pipe_params_t *params, uint32_t grid, uint32_t cta_threads,
@@ -290,4 +456,42 @@ extern "C" int pb_dev_label_ws_occupancy(uint32_t cta_threads, uint32_t smem_byt
                                                          smem_bytes) == cudaSuccess
                ? 0
                : -1;
+}
+
+extern "C" uint32_t pb_wsg_smem_bytes(uint32_t csm, uint32_t g_log2, uint32_t team_warps)
+{
+    const uint32_t nthr = 32u * team_warps, slots = nthr >> g_log2;
+    return (2u * (1u << g_log2) * csm + 3u * 2u * slots + 2u * 6u * nthr + 3u) * 16u;
+}
+
+extern "C" int pb_dev_label_wsg(const pb_wsg_params_t *params, uint32_t grid, uint32_t cta_threads,
+                                uint32_t smem_bytes, cudaStream_t stream)
+{
+    if (params->g_log2 > 2 || (params->team_warps != 7 && params->team_warps != 15) ||
+        cta_threads != 32u * (params->team_warps + 1) ||
+        smem_bytes < pb_wsg_smem_bytes(params->topo.csm, params->g_log2, params->team_warps))
+        return -1;
+    cudaGetLastError(); /* report only this launch */
+    pb::k_label_wsg<<<grid, cta_threads, smem_bytes, stream>>>(*params);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+/* Allow k_label_wsg the largest dynamic shared memory a CTA can have (the
+ * device's opt-in limit less the kernel's static shared memory) and report
+ * it; call before capturing a launch (the attribute is per function, not per
+ * launch). */
+extern "C" int pb_dev_label_wsg_prepare(uint32_t *max_smem_bytes)
+{
+    int dev = 0, optin = 0;
+    cudaFuncAttributes fa;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, pb::k_label_wsg) != cudaSuccess)
+        return -1;
+    const int lim = optin - (int)fa.sharedSizeBytes;
+    if (lim <= 0 || cudaFuncSetAttribute(pb::k_label_wsg, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) !=
+                        cudaSuccess)
+        return -1;
+    if (max_smem_bytes) *max_smem_bytes = (uint32_t)lim;
+    return 0;
 }

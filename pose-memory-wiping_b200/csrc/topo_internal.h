@@ -34,6 +34,11 @@ int pb_plan_for_budget(const pose_hbm_topo_t *t, uint64_t nunits, uint64_t budge
 int pb_topo_label_raw(const pose_hbm_topo_t *t, const uint8_t *chunk_seeds, void *hbm_dev_ptr,
                       size_t hbm_len, const pose_b200_sched_t *sched, pose_b200_stats_t *stats);
 
+/* The pipelined records for a 512-slot shared pool per unit (built on the
+ * first call and kept with the topology), for the multi-unit depth kernel.
+ * Needs a topology built with its block-0 table.  Returns 0 or -1. */
+int pb_topo_view2_small(const pose_hbm_topo_t *t, pb_topo_view2_t *out);
+
 /* Passes a team of T warps makes over all levels running G units in lockstep. */
 uint64_t pb_topo_passes(const pose_hbm_topo_t *t, uint32_t T, uint32_t G);
 /* Free device memory usable for scratch under an optional cap (the topology's

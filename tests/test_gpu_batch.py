@@ -116,6 +116,44 @@ def test_deep_requests_run_as_a_second_launch(pkg, cuda):
             t.free()
 
 
+@pytest.mark.parametrize("deep_cb,shallow_cb,units", [(4096, 256, "1"), (4096, 256, "2"), (4096, 256, "4"),
+                                                     (3000, 100, "4")])
+def test_multi_unit_depth_kernel_writes_the_same_bytes(pkg, cuda, monkeypatch, deep_cb, shallow_cb, units):
+    """The deep part on the multi-unit depth kernel with 1, 2 or 4 units per
+    CTA (a ragged last batch, levels wider than the staged slots, session
+    seeds of several lengths) writes what single calls and the lockstep
+    kernel write."""
+    rnd = random.Random(deep_cb + int(units))
+    topos = {cb: pkg.Topology(cb) for cb in (deep_cb, shallow_cb)}
+    try:
+        reqs, bufs = [], []
+        for i, ns in enumerate([1, 2, 1, 3, 2, 2, 1]):  # 9 deep chunks = 18 units
+            cb = deep_cb if i < 5 else shallow_cb
+            key = rnd.randbytes([32, 0, 9, 200, 32, 32, 5][i])
+            nbytes = ns * cb * 32 + (17 if i == 2 else 0)
+            buf = cuda.zeros(nbytes, dtype=cuda.uint8, device="cuda")
+            reqs.append((topos[cb], key, buf.data_ptr(), nbytes, cb * rnd.randrange(1 << 20)))
+            bufs.append(buf)
+        got = {}
+        for kernel in ("1", "0"):
+            monkeypatch.setenv("POSE_B200_DEEP_UNITS", units)
+            monkeypatch.setenv("POSE_B200_DEEP_KERNEL", kernel)
+            for t in bufs:
+                t.fill_(0x6B)
+            with pkg.Batch(reqs) as b:
+                rc, st = b.run()
+            assert rc == 0 and st["kernel_launches"] == 4, (kernel, st)
+            got[kernel] = [t.cpu().numpy().tobytes() for t in bufs]
+        assert got["1"] == got["0"]
+        for (topo, key, ptr, nbytes, rbo), data in zip(reqs, got["1"]):
+            ref = cuda.full((nbytes,), 0x6B, dtype=cuda.uint8, device="cuda")
+            assert topo.label(key, ref.data_ptr(), nbytes, rbo) == 0
+            assert ref.cpu().numpy().tobytes() == data
+    finally:
+        for t in topos.values():
+            t.free()
+
+
 def test_batched_256_sessions_sampled_vs_reference(pkg, cuda, wl):
     rows = {r["session"]: r for r in golden("configs.json")["batched_sampled"]}
     sessions = wl.batched()
