@@ -35,7 +35,7 @@ typedef struct {
 #define POSE_B200_PACK_CHAIN 255u
 /* flags: run every request of a batch in one launch.  Without it, a batch
  * whose deepest topologies are much deeper than the rest runs them as a
- * second, concurrent launch of 8-warp teams. */
+ * second, concurrent launch (see pose_b200_batch_create). */
 #define POSE_B200_BATCH_ONE_LAUNCH 1u
 
 /* What one call did (device times from CUDA events on the labeler's stream). */
@@ -125,9 +125,15 @@ typedef struct pose_b200_batch pose_b200_batch_t;
  * by the makespan estimate.  Deep part: the requests whose topology's chain
  * (passes of an 8-warp team over one chunk copy) is at least 3/4 of the
  * deepest, when the others are shallower, run as a second launch captured
- * beside the first (8-warp teams, units packed up to 4 a team so that they
- * hold about half the SMs' team slots) unless flags has
- * POSE_B200_BATCH_ONE_LAUNCH; sched then applies to the rest. */
+ * beside the first unless flags has POSE_B200_BATCH_ONE_LAUNCH; sched then
+ * applies to the rest.  When the deep requests share one topology built with
+ * its block-0 table, that launch is the multi-unit depth kernel (1, 2 or 4
+ * chunk copies per CTA, at most one CTA per SM; the topology then also keeps
+ * a second set of pipelined records, 32 bytes per node, built on first use).
+ * Otherwise it is the lockstep kernel with 8-warp teams, units packed up to
+ * 4 a team so that they hold about half the SMs' team slots.  The
+ * environment variable POSE_B200_DEEP_KERNEL=0 selects the lockstep kernel
+ * in every case. */
 pose_b200_batch_t *pose_b200_batch_create(const pose_b200_request_t *reqs, size_t n,
                                           const pose_b200_sched_t *sched);
 /* The empirical autotuner: rank the schedules sched leaves open (team size
