@@ -609,9 +609,7 @@ no_split:
                 wsg = grid * ((uint64_t)v2.gpool * 32 << glog) <= budget;
             }
             if (wsg) {
-                const char *ex = getenv("POSE_B200_DEEP_EXCLUSIVE");
-                uint32_t smem = pb_wsg_smem_bytes(v2.csm, glog, 15);
-                if (ex && ex[0] == '1') smem = 0xFFFFFFFFu; /* the most a CTA can have: no other CTA fits beside it */
+                const uint32_t smem = pb_wsg_smem_bytes(v2.csm, glog, 15);
                 if (pb_plan_requests(pd, nd, 8, 1, 0.9999, &pl[1]) != 0 || pl[1].nunits == 0) goto fail;
                 if (part_setup_wsg(b, &b->part[1], &pl[1], &v2, glog, sms, smem) != 0) goto fail;
             } else {
