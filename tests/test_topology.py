@@ -207,7 +207,9 @@ def pipelined(L, cb, csm):
 
 
 @pytest.mark.parametrize("cb,csm", [(1, 4), (3, 2), (16, 4), (100, 16), (1024, 64), (1024, 4096),
-                                    (4096, 32), (4096, 2048)])
+                                    (4096, 32), (4096, 2048),
+                                    # the multi-unit depth kernel's 512-slot pools
+                                    (3000, 512), (4096, 512), (16384, 512)])
 def test_pipelined_records_are_safe(host, cb, csm):
     """Simulate the pipelined schedule level by level with both pools:
     every read sees its predecessor, no slot is written while it is read in the
