@@ -26,6 +26,10 @@
  * Items beyond the first NC*32 of a wide level are hashed with direct loads.
  * No thread waits on anything but its own cp.async groups and the CTA
  * barrier: there are no spin-waits.
+ *
+ * k_label_wsg is the same design for up to four chunk copies of one topology
+ * per CTA (the deep part of a batch): records are staged once for all units,
+ * and each unit has its own shared-memory pool, built for 512 slots.
  */
 #include "b3_device.cuh"
 #include "kernels.h"
