@@ -7,7 +7,7 @@
 # bench calls resolves to this library and nothing clashes.
 # Usage: oracle/link_disk_wipe_bench.sh <out-dir>
 set -e
-REF=${REF:-/root/reference}
+REF=${POSE_REF:-${REF:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 ROOT=$(dirname "$HERE")
 OUT=${1:-$HERE/_ref}

@@ -53,6 +53,15 @@ static void set_err(const char *fmt, ...)
 
 const char *pose_b200_last_error(void) { return g_err; }
 
+void pb_set_err(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    fprintf(stderr, "%s\n", g_err);
+}
+
 static int quiet(void)
 {
     const char *e = getenv("POSE_GPU_QUIET");
@@ -99,6 +108,7 @@ struct pose_hbm_topo {
      * multi-unit depth kernel's), built on first use */
     void *d_recs2s;
     pb_topo_view2_t view2s;
+    pthread_mutex_t lazy_mu; /* guards the first-use build of d_recs2s / view2s */
     /* schedule chosen by pose_b200_topo_autotune for calls of tuned_units chunk copies */
     int tuned_ok;
     uint64_t tuned_units;
@@ -392,6 +402,7 @@ void pose_graph_hbm_topo_free(pose_hbm_topo_t *t)
     if (prev >= 0 && prev != t->device) cudaSetDevice(prev);
     free(t->wval);
     free(t->wcnt);
+    pthread_mutex_destroy(&t->lazy_mu);
     free(t);
 }
 
@@ -417,6 +428,7 @@ static pose_hbm_topo_t *pose_b200_topo_build_impl(uint32_t chunk_blocks, int wit
     pose_hbm_topo_t *t = (pose_hbm_topo_t *)calloc(1, sizeof(*t));
     uint32_t *ws = NULL;
     if (!t) { set_err("pose_graph_hbm_topo_build: out of host memory"); goto fail_host; }
+    pthread_mutex_init(&t->lazy_mu, NULL);
     cudaGetDevice(&t->device);
     t->cb = cb;
     t->super_bytes = (uint64_t)cb * 32;
@@ -511,7 +523,7 @@ fail:
 fail_host:
     free(ws);
     pb_topo_host_free(&h);
-    if (t) { free(t->wval); free(t->wcnt); free(t); }
+    if (t) { free(t->wval); free(t->wcnt); pthread_mutex_destroy(&t->lazy_mu); free(t); }
     return NULL;
 }
 
@@ -1112,9 +1124,15 @@ int pb_topo_view2_small(const pose_hbm_topo_t *ct, pb_topo_view2_t *out)
 {
     pose_hbm_topo_t *t = (pose_hbm_topo_t *)ct; /* the record set is built once and kept */
     if (!t || !out || !t->d_cv0 || !t->d_recs2) return -1;
+    /* several host threads may create batches on one topology at once: the
+     * first one builds the records, the others wait for it and reuse them */
+    pthread_mutex_lock(&t->lazy_mu);
     if (!t->d_recs2s) {
         pb_topo_host_t h;
-        if (pb_topo_host_build_ex(t->cb, PB_CSM_MULTI, &h) != 0) return -1;
+        if (pb_topo_host_build_ex(t->cb, PB_CSM_MULTI, &h) != 0) {
+            pthread_mutex_unlock(&t->lazy_mu);
+            return -1;
+        }
         /* the same levels and node order as the default records; only the
          * pool slots differ */
         int ok = h.recs2 && h.S == t->S && h.L == t->L;
@@ -1136,9 +1154,13 @@ int pb_topo_view2_small(const pose_hbm_topo_t *ct, pb_topo_view2_t *out)
         }
         if (prev >= 0 && prev != t->device) cudaSetDevice(prev);
         pb_topo_host_free(&h);
-        if (!ok) return -1;
+        if (!ok) {
+            pthread_mutex_unlock(&t->lazy_mu);
+            return -1;
+        }
     }
     *out = t->view2s;
+    pthread_mutex_unlock(&t->lazy_mu);
     return 0;
 }
 

@@ -609,6 +609,13 @@ no_split:
                 wsg = grid * ((uint64_t)v2.gpool * 32 << glog) <= budget;
             }
             if (wsg) {
+                /* a device whose CTAs cannot hold the kernel's shared memory
+                 * keeps the deep part on the lockstep kernel */
+                uint32_t max_smem = 0;
+                wsg = pb_dev_label_wsg_prepare(&max_smem) == 0 && pb_wsg_smem_bytes(v2.csm, glog, 15) <= max_smem;
+                cudaGetLastError();
+            }
+            if (wsg) {
                 const uint32_t smem = pb_wsg_smem_bytes(v2.csm, glog, 15);
                 if (pb_plan_requests(pd, nd, 8, 1, 0.9999, &pl[1]) != 0 || pl[1].nunits == 0) goto fail;
                 if (part_setup_wsg(b, &b->part[1], &pl[1], &v2, glog, sms, smem) != 0) goto fail;

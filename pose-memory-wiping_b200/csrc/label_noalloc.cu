@@ -8,8 +8,8 @@
  * cudaMalloc while they label: a wipe worker that reserved the device's free
  * memory for its label window up front (an allocation there could fail
  * half-way through a disk, or land in memory another tenant is about to
- * claim), or a host that runs the labeler while stream capture or a
- * foreign allocator forbids new allocations.  The topology (an input built
+ * claim), or a host whose own memory pool already holds the device's memory.
+ * The topology (an input built
  * earlier by pose_graph_hbm_topo_build), the session seed and the output
  * buffer still come from the caller.
  *
@@ -26,7 +26,6 @@
 
 #include <cuda_runtime.h>
 #include <pthread.h>
-#include <stdio.h>
 #include <string.h>
 
 #define PB_NOALLOC_SCRATCH_BYTES (64ull << 20)
@@ -83,26 +82,25 @@ extern "C" int pose_b200_topo_label_noalloc(const pose_hbm_topo_t *topo, const u
 {
     pb_topo_internal_t ti;
     if (pb_topo_internal(topo, &ti) != 0) {
-        fprintf(stderr, "pose_b200_topo_label_noalloc: NULL topology\n");
+        pb_set_err("pose_b200_topo_label_noalloc: NULL topology");
         return -1;
     }
     const uint64_t num_super = hbm_len / ti.super_bytes;
     if (num_super == 0) return 0; /* smaller than one super-chunk: nothing to label */
     if (!hbm_dev_ptr || (!session_seed && seed_len)) {
-        fprintf(stderr, "pose_b200_topo_label_noalloc: NULL buffer or seed\n");
+        pb_set_err("pose_b200_topo_label_noalloc: NULL buffer or seed");
         return -1;
     }
     if (seed_len > PB_NOALLOC_MAX_SEED) {
-        fprintf(stderr,
-                "pose_b200_topo_label_noalloc: session seed of %zu bytes exceeds the %u-byte maximum "
-                "of the no-allocation entry point\n",
-                seed_len, PB_NOALLOC_MAX_SEED);
+        pb_set_err("pose_b200_topo_label_noalloc: session seed of %zu bytes exceeds the %u-byte maximum "
+                   "of the no-allocation entry point",
+                   seed_len, PB_NOALLOC_MAX_SEED);
         return -1;
     }
     int prev = -1;
     cudaGetDevice(&prev);
     if (prev != ti.device && cudaSetDevice(ti.device) != cudaSuccess) {
-        fprintf(stderr, "pose_b200_topo_label_noalloc: cannot select the topology's device\n");
+        pb_set_err("pose_b200_topo_label_noalloc: cannot select the topology's device");
         return -1;
     }
     int rc = -1;
@@ -111,15 +109,14 @@ extern "C" int pose_b200_topo_label_noalloc(const pose_hbm_topo_t *topo, const u
     const uint64_t per_launch = num_super < PB_NOALLOC_MAX_CHUNKS ? num_super : PB_NOALLOC_MAX_CHUNKS;
     cudaStream_t s = ti.stream;
     if (na_setup(ti.device, &na) != 0) {
-        fprintf(stderr, "pose_b200_topo_label_noalloc: cudaGetSymbolAddress failed: %s\n",
-                cudaGetErrorString(cudaGetLastError()));
+        pb_set_err("pose_b200_topo_label_noalloc: cudaGetSymbolAddress failed: %s",
+                   cudaGetErrorString(cudaGetLastError()));
         goto out;
     }
     if (pb_plan_for_budget(topo, per_launch * ti.copies, PB_NOALLOC_SCRATCH_BYTES, &plan) != 0) {
-        fprintf(stderr,
-                "pose_b200_topo_label_noalloc: chunk_blocks %u needs %llu bytes of scratch per chunk copy, "
-                "more than the %llu bytes the no-allocation entry point holds\n",
-                ti.cb, (unsigned long long)ti.view.pool * 32ull, PB_NOALLOC_SCRATCH_BYTES);
+        pb_set_err("pose_b200_topo_label_noalloc: chunk_blocks %u needs %llu bytes of scratch per chunk copy, "
+                   "more than the %llu bytes the no-allocation entry point holds",
+                   ti.cb, (unsigned long long)ti.view.pool * 32ull, PB_NOALLOC_SCRATCH_BYTES);
         goto out;
     }
     if (seed_len && cudaMemcpyAsync(na.session, session_seed, seed_len, cudaMemcpyHostToDevice, s) != cudaSuccess)
@@ -158,7 +155,7 @@ extern "C" int pose_b200_topo_label_noalloc(const pose_hbm_topo_t *topo, const u
     rc = 0;
     goto out;
 cuda_fail:
-    fprintf(stderr, "pose_b200_topo_label_noalloc: CUDA error: %s\n", cudaGetErrorString(cudaGetLastError()));
+    pb_set_err("pose_b200_topo_label_noalloc: CUDA error: %s", cudaGetErrorString(cudaGetLastError()));
     /* a call that stopped part way clears all three arrays, best effort */
     cudaMemsetAsync(na.scratch, 0, PB_NOALLOC_SCRATCH_BYTES, s);
     cudaMemsetAsync(na.seeds, 0, sizeof(g_na_seeds), s);

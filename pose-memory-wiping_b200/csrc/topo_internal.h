@@ -26,6 +26,9 @@ typedef struct {
 } pb_plan_out_t;
 
 int pb_topo_internal(const pose_hbm_topo_t *t, pb_topo_internal_t *out);
+/* Record a calling thread's error message for pose_b200_last_error() and
+ * print it to stderr, as every public entry point does on failure. */
+void pb_set_err(const char *fmt, ...);
 /* The automatic schedule for nunits chunk copies within a fixed scratch budget. */
 int pb_plan_for_budget(const pose_hbm_topo_t *t, uint64_t nunits, uint64_t budget, pb_plan_out_t *out);
 

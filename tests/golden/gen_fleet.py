@@ -14,7 +14,8 @@ import os
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/tools/disk-calc/disk_calc.py"
+REF_ROOT = os.environ.get("POSE_REF", "/root/reference")  # the reference tree; override with POSE_REF
+REF = os.path.join(REF_ROOT, "tools", "disk-calc", "disk_calc.py")
 
 TB = 1e12
 CASES = [

@@ -33,7 +33,8 @@ import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF_TEST_HASH = "/root/reference/common/test/test_hash.c"
+REF_ROOT = os.environ.get("POSE_REF", "/root/reference")  # the reference tree; override with POSE_REF
+REF_TEST_HASH = os.path.join(REF_ROOT, "common", "test", "test_hash.c")
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 from oracle import RefCPU  # noqa: E402

@@ -11,7 +11,8 @@ import pytest
 
 from conftest import PKG_DIR, ROOT
 
-REF = "/root/reference/tools/disk-wipe-bench/disk_wipe_bench.cu"
+REF_ROOT = os.environ.get("POSE_REF", "/root/reference")  # the reference tree; override with POSE_REF
+REF = os.path.join(REF_ROOT, "tools", "disk-wipe-bench", "disk_wipe_bench.cu")
 
 
 @pytest.mark.skipif(not os.path.exists(REF), reason="reference sources not present")
