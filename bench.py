@@ -159,14 +159,15 @@ def profiled_traffic(workload_name: str, kernel: int) -> float | None:
 # ── reference CPU leg ───────────────────────────────────────────────────────
 
 def cpu_reference(w: dict, steps: int, warmup: int, cores: int | None = None) -> dict:
-    """Time the reference's own CPU in-place labeler (oracle/_ref) on a
-    bounded sample: one super-chunk per host thread per step."""
+    """Time the reference's own CPU in-place labeler (oracle/_ref) on the
+    whole workload: every step labels all of its super-chunks, spread over
+    every host thread (waves of one super-chunk per thread)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import RefCPU  # test infrastructure: the reference's CPU labeler, CPU legs only
     ref = RefCPU()
     cores = cores or os.cpu_count() or 1
     cb = w["chunk_blocks"]
-    n = min(w["chunks"], cores)
+    n = w["chunks"]
     times = []
     for i in range(warmup + steps):
         t0 = time.perf_counter()
@@ -176,9 +177,33 @@ def cpu_reference(w: dict, steps: int, warmup: int, cores: int | None = None) ->
             times.append(dt)
     sec = sum(times) / len(times)
     return {"value": n * cb * 32 / MIB / sec, "unit": "MiB/s", "cores": cores, "kind": "reference",
-            "sample": f"{n} super-chunks of chunk_blocks={cb} per step ({n * w['nodes_per_chunk']:.3g} nodes), "
-                      f"{steps} timed steps, one chunk per host thread",
+            "sample": f"the whole workload per step: {n} super-chunks of chunk_blocks={cb} "
+                      f"({n * w['nodes_per_chunk']:.3g} nodes) on {cores} host threads, {steps} timed steps",
             "seconds_per_step": sec}
+
+
+def golden_parity(w: dict, rbo: int, nsup: int, data) -> dict:
+    """Compare the persisted super-chunks in `data` (host bytes, nsup
+    super-chunks from block offset rbo) with the reference's digests in
+    tests/golden/configs.json (made by the reference's own CPU labeler):
+    'bit-exact' when every covered super-chunk matches, 'mismatch' otherwise,
+    'unchecked' when no digest covers this range."""
+    import hashlib
+    path = os.path.join(ROOT, "tests", "golden", "configs.json")
+    g = json.load(open(path)).get(w["name"].split(" ")[0]) if os.path.exists(path) else None
+    cb = w["chunk_blocks"]
+    sb = cb * 32
+    if not g or g["key"] != w["key"].hex() or g["chunk_blocks"] != cb or (rbo - g["rbo"]) % cb:
+        return {"parity": "unchecked", "checked_super_chunks": 0}
+    first = (rbo - g["rbo"]) // cb
+    digests = g["super_chunk_sha256"]
+    idx = [j for j in range(nsup) if 0 <= first + j < len(digests)]
+    if not idx:
+        return {"parity": "unchecked", "checked_super_chunks": 0}
+    mv = memoryview(data)
+    bad = [j for j in idx if hashlib.sha256(mv[j * sb:(j + 1) * sb]).hexdigest() != digests[first + j]]
+    return {"parity": "mismatch" if bad else "bit-exact", "checked_super_chunks": len(idx),
+            "mismatched_super_chunks": bad[:8]}
 
 
 def run_reference_arm(args) -> None:
@@ -201,7 +226,46 @@ def run_reference_arm(args) -> None:
                        "parallelism": "host threads"},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": "MiB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if w["name"] == "plain_2e17" and not args.no_aux:
+        line["reference_gpu_warp_sm100"] = reference_gpu_warp(w)
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_warp(w: dict) -> dict:
+    """The reference's own CUDA "warp" strategy built for sm_100 from its
+    sources (oracle/_ref/libposeref_warp.so, `make -C oracle ref_gpu`), timed
+    on this GPU by oracle/ref_gpu_bench.py in its own process (it exports the
+    same C symbols as libpose_b200.so): the workload's 32 super-chunks with
+    their digests checked, and the reference's default 16 GiB window."""
+    so = os.path.join(ROOT, "oracle", "_ref", "libposeref_warp.so")
+    if not os.path.exists(so):
+        return {"unavailable": "oracle/_ref/libposeref_warp.so not built"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU"}
+    except ImportError:
+        return {"unavailable": "torch absent"}
+    out = {"build": "common/src/cuda label_gpu_common.cu + label_gpu_warp.cu + blake3_node.cu, "
+                    "-gencode arch=compute_100,code=sm_100, POSE_GPU_WARP_MIN_BLOCKS=3"}
+    script = os.path.join(ROOT, "oracle", "ref_gpu_bench.py")
+    for name, chunks, extra in (("plain_2e17", w["chunks"], ["--check", "--reps", "2"]),
+                                ("window_2e17", 4096, ["--reps", "1"])):
+        try:
+            with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+                r = subprocess.run([sys.executable, script, "--chunks", str(chunks), "--chunk-blocks",
+                                    str(w["chunk_blocks"]), *extra], capture_output=True, text=True, timeout=600,
+                                   env=dict(os.environ, POSE_GPU_QUIET="1"))
+            lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+            if r.returncode != 0 or not lines:
+                out[name] = {"unavailable": f"rc={r.returncode}: {r.stderr.strip()[-300:]}"}
+                continue
+            d = json.loads(lines[-1])
+            d["clocks"] = clk.summary()
+            out[name] = d
+        except subprocess.TimeoutExpired:
+            out[name] = {"unavailable": "timed out after 600 s"}
+    return out
 
 
 # ── B200 arm ────────────────────────────────────────────────────────────────
@@ -224,6 +288,10 @@ def run_window(pkg, torch, topo, rate: float, reps: int = 1) -> dict:
         assert rc == 0, pkg.last_error()
         if best is None or st["total_ms"] < best["total_ms"]:
             best = st
+    # its first 32 super-chunks are the plain workload's: check them against
+    # the reference's digests
+    first = 32 * w["chunk_blocks"] * 32
+    par = golden_parity(dict(w, name="plain_2e17"), 0, 32, buf[:first].cpu().numpy())
     del buf
     comps = 2 if best["used_cv0_table"] else 3
     achieved = best["nodes"] * comps * 680.0 / (best["kernel_ms"] * 1e-3)
@@ -235,7 +303,53 @@ def run_window(pkg, torch, topo, rate: float, reps: int = 1) -> dict:
                          "chosen_by": "pose_b200_topo_autotune (10 timed trials)"},
             "roofline": {"bound": "int32", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s",
                          "frac": achieved / peak,
-                         "frac_of_spec_method": best["nodes"] * 3 * 680.0 / (best["kernel_ms"] * 1e-3) / peak}}
+                         "ops_per_node": comps * 680.0},
+            "parity": par["parity"], "parity_checked_super_chunks": par["checked_super_chunks"]}
+
+
+def run_plain_leg(pkg, torch, name: str, rate: float, lat_cycles: float, warm: int = 1, reps: int = 2) -> dict:
+    """One more plain workload through pose_graph_hbm_topo_label with its
+    topology resident (its scratch cap, if any, on every call): best of
+    `reps` timed calls after `warm` untimed ones, its bytes checked against
+    the reference's digests, clocks sampled during the timed calls."""
+    w = workload(name)
+    cb, nsup = w["chunk_blocks"], w["chunks"]
+    nbytes = nsup * cb * 32
+    cap = pkg.Sched(scratch_cap_bytes=w["scratch_cap_bytes"]) if w.get("scratch_cap_bytes") else None
+    topo = pkg.Topology(cb)
+    buf = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    for _ in range(warm):
+        assert topo.label(w["key"], buf.data_ptr(), nbytes, w["rbo"], sched=cap) == 0, pkg.last_error()
+    best = None
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        for _ in range(reps):
+            rc, st = topo.label(w["key"], buf.data_ptr(), nbytes, w["rbo"], sched=cap, stats=True)
+            assert rc == 0, pkg.last_error()
+            if best is None or st["total_ms"] < best["total_ms"]:
+                best = st
+    torch.cuda.synchronize()
+    par = golden_parity(w, w["rbo"], nsup, buf.cpu().numpy())
+    levels = topo.info()["levels"]
+    topo.free()
+    del buf
+    comps = 2 if best["used_cv0_table"] else 3
+    clocks = clk.summary()
+    sm_hz = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    t_depth = levels * comps * lat_cycles / sm_hz
+    achieved = best["nodes"] * comps * 680.0 / (best["kernel_ms"] * 1e-3)
+    out = {"workload": f"{name}: {nsup} super-chunks of chunk_blocks {cb}, key splitmix64",
+           "value": nbytes / MIB / (best["total_ms"] * 1e-3), "unit": "MiB/s", "ms": best["total_ms"],
+           "kernel_ms": best["kernel_ms"], "kernel": best["kernel"],
+           "schedule": {"T": best["team_warps"], "G": best["units_per_team"], "teams": best["teams"],
+                        "scratch_bytes": best["scratch_bytes"]},
+           "scratch_cap_bytes": w.get("scratch_cap_bytes"),
+           "roofline": {"bound": "int32", "achieved": achieved / 1e12, "peak": rate * 680.0 / 1e12,
+                        "unit": "Tops/s", "frac": achieved / (rate * 680.0),
+                        "depth_bound_mib_s": nbytes / MIB / t_depth,
+                        "depth_frac": t_depth * 1e3 / best["kernel_ms"]},
+           "clocks": clocks}
+    out.update(par)
+    return out
 
 
 def run_batched(pkg, torch, sched=None, reps: int = 2) -> dict:
@@ -411,6 +525,10 @@ def run_b200(args) -> None:
             e2e_times.append(time.perf_counter() - t0)
             assert rc == 0
         barrier()
+    # the bytes of the last timed call and of the last end-to-end host copy,
+    # against the reference's digests
+    par_dev = golden_parity(w, rbo, nsup, buf.cpu().numpy())
+    par_host = golden_parity(w, rbo, nsup, host.numpy())
     device_ms = sum(s["total_ms"] for s in stats)
     kernel_ms = sum(s["kernel_ms"] for s in stats) / len(stats)
     e2e_s = sum(e2e_times) / len(e2e_times)
@@ -460,17 +578,26 @@ def run_b200(args) -> None:
                      "compress_latency_cycles": lat_cycles},
         "e2e": {"value": e2e_value, "unit": "MiB/s", "h2d_bytes_per_step": len(w["key"]),
                 "d2h_bytes_per_step": nbytes},
+        "parity": "mismatch" if "mismatch" in (par_dev["parity"], par_host["parity"]) else par_dev["parity"],
+        "parity_checked": {"timed_output": par_dev, "e2e_host_copy": par_host,
+                           "against": "tests/golden/configs.json: per-super-chunk SHA-256 of the reference's "
+                                      "own CPU labeler on the same key and positions (rank 0's range)"},
         "gpu_launches": int(sum(2 * s["kernel_launches"] for s in stats)),
         "clocks": clocks,
         "kernel_ms": kernel_ms,
     }
     if world == 1 and not args.no_aux and args.workload == "plain_2e17":
-        line["window_2e17"] = run_window(pkg, torch, topo, rate)
-        line["batched"] = run_batched(pkg, torch)
-        line["served"] = run_served(pkg, torch, requests=120, alone=True)
+        for key, fn in (("window_2e17", lambda: run_window(pkg, torch, topo, rate)),
+                        ("batched", lambda: run_batched(pkg, torch)),
+                        ("served", lambda: run_served(pkg, torch, requests=120, alone=True))):
+            with ClockSampler(local) as aclk:
+                line[key] = fn()
+            line[key]["clocks"] = aclk.summary()
+        line["deep_2e20"] = run_plain_leg(pkg, torch, "deep_2e20", rate, lat_cycles, warm=1, reps=2)
+        line["plain_small"] = run_plain_leg(pkg, torch, "plain_small", rate, lat_cycles, warm=3, reps=5)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_reference(w, 1, 0)
+            cpu = cpu_reference(w, 3, 1)
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as exc:  # the oracle's reference build may be absent
             line["cpu_baseline"] = {"value": None, "unit": "MiB/s", "cores": os.cpu_count(), "kind": "reference",
@@ -481,6 +608,8 @@ def run_b200(args) -> None:
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+    if line["parity"] == "mismatch":
+        raise SystemExit("bench: labels differ from the reference's digests")
 
 
 def run_aux(args) -> None:

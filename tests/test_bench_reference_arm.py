@@ -45,3 +45,26 @@ def test_reference_arm_is_silent_on_other_ranks():
     r = _run({"RANK": "1", "WORLD_SIZE": "2"}, "--workload", "plain_small", "--steps", "1", "--warmup", "3")
     assert r.returncode == 0, r.stderr[-2000:]
     assert not [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+
+
+def test_bench_parity_check_against_reference_digests():
+    """bench.py hashes the bytes it timed against the reference's digests:
+    the reference CPU labeler's own output of the small plain workload reads
+    bit-exact, a planted byte flip (in that host copy) reads mismatch, and a
+    range no digest covers reads unchecked."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    bench.load_pkg()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import RefCPU
+    w = bench.workload("plain_small")
+    data = RefCPU().label_super_chunks(w["key"], w["chunk_blocks"], w["chunks"], w["rbo"])
+    ok = bench.golden_parity(w, w["rbo"], w["chunks"], data)
+    assert ok["parity"] == "bit-exact" and ok["checked_super_chunks"] == w["chunks"]
+    data[5 * w["chunk_blocks"] * 32 + 17] ^= 1
+    bad = bench.golden_parity(w, w["rbo"], w["chunks"], data)
+    assert bad["parity"] == "mismatch" and bad["mismatched_super_chunks"] == [5]
+    far = w["rbo"] + 10_000 * w["chunk_blocks"]
+    assert bench.golden_parity(w, far, w["chunks"], data)["parity"] == "unchecked"
