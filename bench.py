@@ -388,7 +388,7 @@ def run_batched(pkg, torch, sched=None, reps: int = 2) -> dict:
                                                  else f"lane efficiency {chosen['lane_efficiency']}%")}
 
 
-def run_served(pkg, torch, requests: int = 300, alone: bool = False) -> dict:
+def run_served(pkg, torch, requests: int = 300, alone: bool = False, rate: float = 200.0) -> dict:
     """Replay a fixed Poisson trace (200 requests/s from 64 sessions,
     chunk_blocks 2^10..2^18, 1-16 chunks each) in real time against the
     continuous-batching server; latency = submit to completion.  With alone,
@@ -397,7 +397,7 @@ def run_served(pkg, torch, requests: int = 300, alone: bool = False) -> dict:
     its measured service time)."""
     import threading
     import pose_b200.workloads as wl
-    trace = wl.served(requests)
+    trace = wl.served(requests, rate_per_s=rate)
     topos = {cb: pkg.Topology(cb) for cb in sorted({r["chunk_blocks"] for r in trace})}
     sizes = [r["chunks"] * r["chunk_blocks"] * 32 for r in trace]
     big = torch.empty(sum(sizes), dtype=torch.uint8, device="cuda")
@@ -430,7 +430,7 @@ def run_served(pkg, torch, requests: int = 300, alone: bool = False) -> dict:
         wall = time.perf_counter() - t0
         st = srv.stats()
     lat_sorted = sorted(lat)
-    out = {"workload": f"served: Poisson 200 req/s, 64 sessions, {len(trace)} requests, chunk_blocks 2^10..2^18",
+    out = {"workload": f"served: Poisson {rate:.4g} req/s, 64 sessions, {len(trace)} requests, chunk_blocks 2^10..2^18",
            "value": sum(sizes) / MIB / wall, "unit": "MiB/s", "p50_ms": lat_sorted[len(lat) // 2],
            "p99_ms": lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))], "waves": st["waves"],
            "offered_mib_s": sum(sizes) / MIB / trace[-1]["arrival_s"], "wall_s": wall}
@@ -593,6 +593,13 @@ def run_b200(args) -> None:
             with ClockSampler(local) as aclk:
                 line[key] = fn()
             line[key]["clocks"] = aclk.summary()
+        # the same trace shape below saturation: arrivals at about 0.7 of the
+        # served rate measured above
+        sv = line["served"]
+        low_rate = 200.0 * 0.7 * sv["value"] / sv["offered_mib_s"]
+        with ClockSampler(local) as aclk:
+            line["served_0p7"] = run_served(pkg, torch, requests=120, rate=low_rate)
+        line["served_0p7"]["clocks"] = aclk.summary()
         line["deep_2e20"] = run_plain_leg(pkg, torch, "deep_2e20", rate, lat_cycles, warm=1, reps=2)
         line["plain_small"] = run_plain_leg(pkg, torch, "plain_small", rate, lat_cycles, warm=3, reps=5)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

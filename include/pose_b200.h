@@ -23,8 +23,9 @@ typedef struct {
     uint32_t team_warps;        /* T: warps that cooperate on one batch (1..16, power of 2) */
     uint32_t units_per_team;    /* G: chunk copies run in lockstep by one team (1..32, power of 2) */
     uint32_t max_teams;         /* cap on resident teams (0 = occupancy and memory bound) */
-    uint32_t kernel;            /* 0 = automatic, 1 = basic lockstep kernel, 2 = pipelined kernel,
-                                   3 = warp-specialised kernel (team_warps = hashing warps: 7 or 15) */
+    uint32_t kernel;            /* 0 = automatic, 1 = basic lockstep kernel,
+                                   3 = warp-specialised depth kernel (team_warps = hashing warps: 7 or 15);
+                                   other values are refused */
     uint64_t scratch_cap_bytes; /* cap on the scratch pool (0 = free HBM less a margin) */
     uint32_t lane_efficiency;   /* batched launches: per-topology G reaches this lane efficiency,
                                    in percent; POSE_B200_PACK_CHAIN packs units while their chain
@@ -48,7 +49,7 @@ typedef struct {
     uint64_t scratch_bytes;     /* scratch pool bytes used */
     uint32_t team_warps, units_per_team, teams, kernel_launches;
     uint32_t used_cv0_table;    /* 1 when block 0 came from the precomputed table */
-    uint32_t kernel;            /* 1 = basic lockstep kernel, 2 = pipelined kernel, 3 = warp-specialised,
+    uint32_t kernel;            /* 1 = basic lockstep kernel, 3 = warp-specialised depth kernel,
                                    4 = multi-topology batch kernel */
 } pose_b200_stats_t;
 

@@ -110,9 +110,8 @@ typedef struct {
     uint32_t desc[8];
 } pb_topo_view2_t;
 
-/* One launch of the pipelined kernel; fields as in pb_label_params_t.  The
- * dynamic shared memory holds teams_per_cta * csm * G labels followed by the
- * staging area (12 x 16 bytes per thread). */
+/* One launch of the depth kernel k_label_ws (label_ws.cu); fields as in
+ * pb_label_params_t, with the pipelined records' view. */
 typedef struct {
     pb_topo_view2_t topo;
     const uint32_t *seeds;
@@ -128,12 +127,6 @@ typedef struct {
     uint32_t nbatches;
     unsigned int *queue;
 } pb_pipe_params_t;
-
-#define PB_PIPE_STAGE_BYTES_PER_THREAD 192u
-
-int pb_dev_label_pipe(const pb_pipe_params_t *params, uint32_t grid, uint32_t cta_threads,
-                      uint32_t smem_bytes, cudaStream_t stream);
-int pb_dev_label_pipe_occupancy(uint32_t cta_threads, uint32_t smem_bytes, int *blocks_per_sm);
 
 /* Warp-specialised depth-regime kernel (label_ws.cu): team_warps hashing
  * warps + 1 producer warp per CTA, one chunk copy per CTA, g_log2 = 0. */

@@ -91,7 +91,6 @@ struct pose_hbm_topo {
     uint64_t dev_bytes;
     pb_topo_view_t view;
     pb_topo_view2_t view2; /* pipelined records (d_recs2 != NULL) */
-    int occ_pipe[5][2];    /* pipelined kernel CTAs/SM for T = 1..16, G = 1, 2 (-1 = not queried) */
     int occ_ws[2];         /* warp-specialised kernel CTAs/SM for 7 and 15 hashing warps */
     /* per-topology workspace, reused across calls (one caller thread at a time) */
     cudaStream_t stream;
@@ -135,13 +134,6 @@ static double model_latency(int cv0)
     return v > 0 ? v : (cv0 ? 6000.0 : 7000.0);
 }
 
-static double model_pipe_latency(void)
-{
-    const char *e = getenv("POSE_B200_PIPE_LATENCY");
-    double v = e ? atof(e) : 0.0;
-    return v > 0 ? v : 2800.0;
-}
-
 typedef struct {
     uint32_t T, G, teams, grid, cta, kernel, smem, fma;
     uint64_t team_scratch, scratch_bytes;
@@ -150,11 +142,6 @@ typedef struct {
 
 #define PB_CSM_LATENCY 2048u /* shared-memory label slots per copy in the pipelined records */
 #define PB_CSM_MULTI 512u    /* the same for the multi-unit depth kernel (four pools per CTA) */
-
-static uint32_t pipe_smem_bytes(const pose_hbm_topo_t *t, uint32_t T, uint32_t G)
-{
-    return t->view2.csm * G * 32u + 32u * T * PB_PIPE_STAGE_BYTES_PER_THREAD;
-}
 
 static double model_ws_latency(void)
 {
@@ -188,19 +175,6 @@ static uint64_t passes_lanes(const pose_hbm_topo_t *t, uint64_t lanes)
     return passes;
 }
 
-static int pipe_occupancy(pose_hbm_topo_t *t, uint32_t T, uint32_t G)
-{
-    int ti = __builtin_ctz(T), gi = G == 1 ? 0 : 1;
-    if (t->occ_pipe[ti][gi] < 0) {
-        int occ = 0;
-        uint32_t smem = pipe_smem_bytes(t, T, G);
-        if (smem > 227u * 1024u || pb_dev_label_pipe_occupancy(32 * T, smem, &occ) != 0) occ = 0;
-        cudaGetLastError();
-        t->occ_pipe[ti][gi] = occ;
-    }
-    return t->occ_pipe[ti][gi];
-}
-
 static uint64_t passes_for(const pose_hbm_topo_t *t, uint32_t T, uint32_t G)
 {
     uint64_t lanes = 32ull * T, passes = 0;
@@ -215,8 +189,8 @@ static int is_pow2(uint32_t v) { return v && !(v & (v - 1)); }
 
 /* Throughput model of one launch.  A team's batch takes at least its
  * latency-bound time (every pass of every level waits for a label: t_lat per
- * pass for the basic kernel; the pipelined kernel's first pass of a level
- * costs t_pipe, further passes t_lat), and an SM needs at least its ALU time
+ * pass for the basic kernel; the depth kernel's levels cost its per-level
+ * time, further passes of a wide level t_lat), and an SM needs at least its ALU time
  * (all node hashes of the teams resident on it at lanes_clk lane-operations
  * per clock).  A launch runs ceil(batches / resident teams) waves of the
  * larger of the two. */
@@ -226,24 +200,21 @@ static int make_plan(const pose_hbm_topo_t *ct, uint64_t nunits, const pose_b200
     pose_hbm_topo_t *t = (pose_hbm_topo_t *)ct; /* occupancy cache */
     const double lanes_clk = model_lanes();
     const double t_lat = model_latency(t->d_cv0 != NULL);
-    const double t_pipe = model_pipe_latency();
     const double item_instr = t->d_cv0 ? 1400.0 : 2080.0;
     const int want = hint ? (int)hint->kernel : 0;
     memset(best, 0, sizeof(*best));
     best->cost = -1;
-    for (int kernel = 1; kernel <= 2; kernel++) {
+    for (int kernel = 1; kernel <= 1; kernel++) {
         if (want && want != kernel) continue;
-        if (want == 0 && kernel == 2 && t->d_recs2) continue; /* superseded by the warp-specialised kernel */
-        if (kernel == 2 && !t->d_recs2) continue;
-        for (uint32_t T = kernel == 2 ? 4 : 1; T <= 16; T <<= 1) {
+        for (uint32_t T = 1; T <= 16; T <<= 1) {
             if (hint && hint->team_warps && hint->team_warps != T) continue;
-            uint32_t cta = kernel == 2 ? 32 * T : (T == 16 ? 512 : 256);
+            uint32_t cta = T == 16 ? 512 : 256;
             uint32_t tpc = cta / (32 * T);
-            for (uint32_t G = 1; G <= 32 && G <= 32 * T && (kernel == 1 || G <= 2); G <<= 1) {
+            for (uint32_t G = 1; G <= 32 && G <= 32 * T; G <<= 1) {
                 if (hint && hint->units_per_team && hint->units_per_team != G) continue;
-                int occ = kernel == 2 ? pipe_occupancy(t, T, G) : (T == 16 ? t->occ512 : t->occ256);
+                int occ = T == 16 ? t->occ512 : t->occ256;
                 if (occ <= 0) continue;
-                uint64_t slots = kernel == 2 ? (t->view2.gpool ? t->view2.gpool : 1) : t->pool;
+                uint64_t slots = t->pool;
                 uint64_t team_scratch = (uint64_t)G * slots * 32;
                 uint64_t batches = (nunits + G - 1) / G;
                 uint64_t cap = (uint64_t)t->sms * occ * tpc;
@@ -258,8 +229,7 @@ static int make_plan(const pose_hbm_topo_t *ct, uint64_t nunits, const pose_b200
                 if (sbytes > budget) continue;
                 uint64_t waves = (batches + R - 1) / R;
                 uint64_t passes = passes_for(t, T, G);
-                double lat = kernel == 2 ? (double)t->L * t_pipe + (double)(passes - t->L) * t_lat
-                                         : (double)passes * t_lat;
+                double lat = (double)passes * t_lat;
                 double teams_sm = (double)((R + t->sms - 1) / t->sms);
                 double alu = teams_sm * G * (double)t->S * item_instr / lanes_clk;
                 double cost = (double)waves * (lat > alu ? lat : alu);
@@ -269,7 +239,7 @@ static int make_plan(const pose_hbm_topo_t *ct, uint64_t nunits, const pose_b200
                     best->grid = (uint32_t)grid; best->cta = cta;
                     best->team_scratch = team_scratch; best->scratch_bytes = sbytes;
                     best->cost = cost; best->kernel = (uint32_t)kernel;
-                    best->smem = kernel == 2 ? pipe_smem_bytes(t, T, G) : 0;
+                    best->smem = 0;
                     best->fma = kernel == 1 && alu >= lat; /* ALU-bound: move adds to the FMA pipe */
                 }
             }
@@ -510,7 +480,6 @@ static pose_hbm_topo_t *pose_b200_topo_build_impl(uint32_t chunk_blocks, int wit
         t->view2.S = h.S; t->view2.L = h.L; t->view2.half_w = h.half_w;
         t->view2.retained = h.retained; t->view2.csm = h.csm; t->view2.gpool = h.gpool2;
         memcpy(t->view2.desc, t->view.desc, sizeof(t->view2.desc));
-        memset(t->occ_pipe, 0xFF, sizeof(t->occ_pipe));
         memset(t->occ_ws, 0xFF, sizeof(t->occ_ws));
     }
     pb_topo_host_free(&h);
@@ -700,6 +669,11 @@ static int topo_label_core_impl(const pose_hbm_topo_t *ct, const uint8_t *sessio
     if (num_super == 0) return 0; /* smaller than one super-chunk: nothing to label */
     if (!hbm_dev_ptr) { set_err("pose_graph_hbm_topo_label: NULL buffer"); return -1; }
     if (!raw_seeds && !session_seed && seed_len) { set_err("pose_graph_hbm_topo_label: NULL seed"); return -1; }
+    if (sched && sched->kernel != 0 && sched->kernel != 1 && sched->kernel != 3) {
+        set_err("pose_b200_topo_label: kernel %u is not one of 0 (automatic), 1 (lockstep) and 3 (depth)",
+                sched->kernel);
+        return -1;
+    }
     if (sched && sched->kernel == 3 && sched->team_warps && sched->team_warps != 7 && sched->team_warps != 15) {
         set_err("pose_b200_topo_label: the warp-specialised kernel takes 7 or 15 hashing warps");
         return -1;
@@ -821,7 +795,7 @@ static int topo_label_core_impl(const pose_hbm_topo_t *ct, const uint8_t *sessio
             { const char *e = getenv("POSE_B200_FMA_ADDS"); if (e && e[0]) p.fma_adds = (uint32_t)atoi(e); }
             CK(cudaEventRecord(t->ev[1], t->stream), "event");
             int lrc;
-            if (plan.kernel == 2 || plan.kernel == 3) {
+            if (plan.kernel == 3) {
                 pb_pipe_params_t pp;
                 memset(&pp, 0, sizeof(pp));
                 pp.topo = t->view2;
@@ -830,8 +804,7 @@ static int topo_label_core_impl(const pose_hbm_topo_t *ct, const uint8_t *sessio
                 pp.team_scratch_bytes = plan.team_scratch; pp.nunits = p.nunits;
                 pp.copies_log2 = p.copies_log2; pp.g_log2 = p.g_log2; pp.team_warps = p.team_warps;
                 pp.nbatches = p.nbatches; pp.queue = p.queue;
-                lrc = plan.kernel == 2 ? pb_dev_label_pipe(&pp, plan.grid, plan.cta, plan.smem, t->stream)
-                                       : pb_dev_label_ws(&pp, plan.grid, plan.cta, plan.smem, t->stream);
+                lrc = pb_dev_label_ws(&pp, plan.grid, plan.cta, plan.smem, t->stream);
             } else {
                 lrc = pb_dev_label(&p, plan.grid, plan.cta, t->stream);
             }
@@ -1118,6 +1091,36 @@ int pb_topo_internal(const pose_hbm_topo_t *t, pb_topo_internal_t *out)
     out->stream = t->stream;
     out->sms = t->sms;
     return 0;
+}
+
+uint64_t pb_topo_depth_unit_scratch(const pose_hbm_topo_t *t)
+{
+    return t && t->d_recs2 && t->d_cv0 ? (uint64_t)(t->view2.gpool ? t->view2.gpool : 1) * 32 : 0;
+}
+
+int pb_topo_launch_depth(const pose_hbm_topo_t *ct, const uint32_t *d_seeds, void *dev_ptr, uint64_t nsuper,
+                         uint8_t *scratch, uint32_t grid, unsigned int *d_queue, cudaStream_t stream)
+{
+    pose_hbm_topo_t *t = (pose_hbm_topo_t *)ct; /* occupancy cache */
+    const uint32_t nc = 15;
+    if (!pb_topo_depth_unit_scratch(t) || nsuper == 0 || grid == 0 || nsuper * t->copies > 0xFFFFFFFFull) return -1;
+    if (ws_occupancy(t, nc) <= 0) return -1;
+    pb_pipe_params_t pp;
+    memset(&pp, 0, sizeof(pp));
+    pp.topo = t->view2;
+    pp.seeds = d_seeds;
+    pp.persist = (uint8_t *)dev_ptr;
+    pp.super_bytes = t->super_bytes;
+    pp.first_super = 0;
+    pp.scratch = scratch;
+    pp.team_scratch_bytes = pb_topo_depth_unit_scratch(t);
+    pp.nunits = (uint32_t)(nsuper * t->copies);
+    pp.copies_log2 = t->copies == 2 ? 1 : 0;
+    pp.g_log2 = 0;
+    pp.team_warps = nc;
+    pp.nbatches = pp.nunits;
+    pp.queue = d_queue;
+    return pb_dev_label_ws(&pp, grid, 32 * (nc + 1), ws_smem_bytes(t, nc), stream);
 }
 
 int pb_topo_view2_small(const pose_hbm_topo_t *ct, pb_topo_view2_t *out)

@@ -20,7 +20,13 @@
  *     system-scope fence), and the dispatcher marks a request done as soon as
  *     all its chunk copies are in, while the rest of its wave still runs;
  *   - finished waves are reaped and their arena range is zeroed on the device
- *     before it is reused.
+ *     before it is reused;
+ *   - deep requests (topologies of at least PB_SERVER_DEEP_LEVELS levels,
+ *     chunk_blocks 2^17 and up) do not join waves: each runs alone on the
+ *     depth kernel (k_label_ws, one chunk copy per CTA, with its own producer
+ *     warp) in a slot of its own, so a wave never waits for a deep request's
+ *     chain and a deep request never runs on the lockstep kernel.  At most one
+ *     depth CTA per SM is in flight; their scratch comes from the same arena.
  * Every request's bytes are those of labelling it alone.
  */
 #include "batch_internal.h"
@@ -37,6 +43,9 @@
 #include <time.h>
 
 #define PB_SERVER_MAX_WAVES 16
+/* Requests whose topology has at least this many levels (chunk_blocks 2^17
+ * and up) run alone on the depth kernel instead of joining a wave. */
+#define PB_SERVER_DEEP_LEVELS 300000u
 
 typedef struct {
     const pose_hbm_topo_t *topo;
@@ -61,6 +70,8 @@ typedef struct {
     unsigned int *h_done;      /* mapped host counters, one per request */
     unsigned int *d_done;
     size_t done_cap;
+    int deep;                  /* one deep request on the depth kernel (completes with the launch) */
+    uint32_t ctas;             /* its CTAs, one SM each */
 } wave_t;
 
 struct pose_b200_server {
@@ -82,7 +93,8 @@ struct pose_b200_server {
     uint64_t free_off[2 * PB_SERVER_MAX_WAVES + 2], free_len[2 * PB_SERVER_MAX_WAVES + 2];
     int nfree;
     wave_t waves[PB_SERVER_MAX_WAVES];
-    uint32_t max_waves;
+    uint32_t max_waves;        /* concurrent multi-topology waves */
+    uint32_t deep_ctas;        /* depth-kernel CTAs in flight */
     int occ;
     uint64_t waves_launched;
     double busy_ms;
@@ -143,16 +155,142 @@ static void arena_give(pose_b200_server_t *s, uint64_t off, uint64_t len)
     }
 }
 
+/* A request that runs alone on the depth kernel: a deep topology that has
+ * the depth kernel's records, whose scratch for one chunk copy fits the
+ * arena (otherwise it joins a wave like the others). */
+static int req_is_deep(const pose_b200_server_t *s, const sreq_t *r)
+{
+    pb_topo_internal_t ti;
+    const uint64_t per = pb_topo_depth_unit_scratch(r->topo);
+    return pb_topo_internal(r->topo, &ti) == 0 && ti.view.L >= PB_SERVER_DEEP_LEVELS && per > 0 &&
+           per <= s->arena_bytes;
+}
+
+/* With the lock held: launch the oldest pending request (a deep one) alone
+ * on the depth kernel, one chunk copy per CTA and CTA per SM, in a free wave
+ * slot.  Its CTAs count against the SMs (at most one depth CTA per SM in
+ * flight) and its scratch comes from the arena.  It completes when its
+ * launch does.  Returns 1 when it was launched (or failed), 0 when it has to
+ * wait for a slot, SMs or scratch. */
+static int admit_deep(pose_b200_server_t *s)
+{
+    const size_t idx = s->next_pending;
+    sreq_t *r = &s->reqs[idx];
+    pb_topo_internal_t ti;
+    if (pb_topo_internal(r->topo, &ti) != 0) return 0;
+    const uint64_t nsuper = r->len / ti.super_bytes;
+    if (nsuper == 0) { /* nothing to label */
+        r->state = 2;
+        r->t_start = r->t_done = now_ms();
+        s->next_pending++;
+        pthread_cond_broadcast(&s->cv);
+        return 1;
+    }
+    int w = -1;
+    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES && w < 0; i++) if (!s->waves[i].busy) w = (int)i;
+    const uint32_t sms = ti.sms > 0 ? (uint32_t)ti.sms : 1;
+    if (w < 0 || s->deep_ctas >= sms) return 0;
+    const uint64_t units = nsuper * ti.copies;
+    uint32_t grid = (uint32_t)(units < sms - s->deep_ctas ? units : sms - s->deep_ctas);
+    const uint64_t per = pb_topo_depth_unit_scratch(r->topo);
+    const uint64_t fit = arena_largest(s) / per;
+    if (fit < grid) grid = (uint32_t)fit;
+    if (grid == 0) return 0; /* wait for scratch */
+    wave_t *wv = &s->waves[w];
+    const uint64_t scratch = (uint64_t)grid * per;
+    uint64_t off = 0;
+    if (arena_take(s, scratch, &off) != 0) return 0;
+    /* tables: jobs | seeds | queue, 256-byte aligned */
+    const size_t o_jobs = 0, o_seeds = (nsuper * sizeof(pb_seedjob_t) + 255) & ~(size_t)255;
+    const size_t o_queue = (o_seeds + nsuper * 32 + 255) & ~(size_t)255, total = o_queue + 256;
+    pb_seedjob_t *jobs = (pb_seedjob_t *)malloc(nsuper * sizeof(pb_seedjob_t));
+    if (!jobs) { arena_give(s, off, scratch); return 0; }
+    if (wv->tables_cap < total) {
+        cudaFree(wv->d_tables);
+        wv->d_tables = NULL;
+        wv->tables_cap = 0;
+        if (pb_dev_malloc(&wv->d_tables, total * 2) != cudaSuccess) {
+            cudaGetLastError();
+            free(jobs);
+            arena_give(s, off, scratch);
+            return 0;
+        }
+        wv->tables_cap = total * 2;
+    }
+    if (wv->reqs_cap < 1) {
+        uint64_t *nr = (uint64_t *)realloc(wv->reqs, sizeof(uint64_t));
+        if (!nr) { free(jobs); arena_give(s, off, scratch); return 0; }
+        wv->reqs = nr;
+        wv->reqs_cap = 1;
+    }
+    for (uint64_t j = 0; j < nsuper; j++) {
+        jobs[j].chunk_index = (r->rbo + j * (uint64_t)ti.cb) / ti.cb;
+        jobs[j].seed_off = s->sess_off[r->session];
+        jobs[j].seed_len = s->sess_len[r->session];
+    }
+    uint8_t *T = (uint8_t *)wv->d_tables;
+    uint32_t *d_seeds = (uint32_t *)(T + o_seeds);
+    int ok = cudaMemcpyAsync(T + o_jobs, jobs, nsuper * sizeof(pb_seedjob_t), cudaMemcpyHostToDevice, wv->stream) ==
+             cudaSuccess;
+    /* the upload reads `jobs`: wait for it before freeing them */
+    ok = ok && cudaStreamSynchronize(wv->stream) == cudaSuccess;
+    free(jobs);
+    ok = ok && pb_dev_seed_jobs(T + o_jobs, (uint32_t)nsuper, s->d_sessions, d_seeds, wv->stream) == 0;
+    ok = ok && cudaMemsetAsync(T + o_queue, 0, 64, wv->stream) == cudaSuccess;
+    ok = ok && pb_topo_launch_depth(r->topo, d_seeds, r->dev_ptr, nsuper, s->d_arena + off, grid,
+                                    (unsigned int *)(T + o_queue), wv->stream) == 0;
+    /* scratch and chunk seeds are zeroed before the request counts as done */
+    ok = ok && cudaMemsetAsync(s->d_arena + off, 0, scratch, wv->stream) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(d_seeds, 0, nsuper * 32, wv->stream) == cudaSuccess;
+    ok = ok && cudaEventRecord(wv->done, wv->stream) == cudaSuccess;
+    const double t = now_ms();
+    if (!ok) {
+        fprintf(stderr, "pose_b200_server: deep launch failed: %s\n", cudaGetErrorString(cudaGetLastError()));
+        cudaStreamSynchronize(wv->stream);
+        cudaMemsetAsync(s->d_arena + off, 0, scratch, wv->stream);
+        cudaMemsetAsync(d_seeds, 0, nsuper * 32, wv->stream);
+        cudaStreamSynchronize(wv->stream);
+        cudaGetLastError();
+        arena_give(s, off, scratch);
+        r->state = 3;
+        r->t_done = t;
+    } else {
+        wv->busy = 1;
+        wv->deep = 1;
+        wv->ctas = grid;
+        wv->arena_off = off;
+        wv->arena_len = scratch;
+        wv->nreqs = 1;
+        wv->reqs[0] = idx;
+        s->deep_ctas += grid;
+        r->state = 1;
+        r->t_start = t;
+        s->waves_launched++;
+    }
+    s->next_pending++;
+    pthread_cond_broadcast(&s->cv);
+    return 1;
+}
+
 /* With the lock held: launch one wave from the oldest pending requests.
  * Returns 1 when a wave was launched, 0 when nothing could be admitted. */
 static int admit(pose_b200_server_t *s)
 {
     if (s->next_pending >= s->nreqs) return 0;
+    if (req_is_deep(s, &s->reqs[s->next_pending])) return admit_deep(s);
     int w = -1;
-    for (uint32_t i = 0; i < s->max_waves; i++) if (!s->waves[i].busy) { w = (int)i; break; }
-    if (w < 0) return 0;
+    uint32_t multi = 0;
+    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
+        if (s->waves[i].busy) multi += !s->waves[i].deep;
+        else if (w < 0) w = (int)i;
+    }
+    if (w < 0 || multi >= s->max_waves) return 0;
     wave_t *wv = &s->waves[w];
-    size_t first = s->next_pending, last = s->nreqs; /* take everything pending */
+    wv->deep = 0;
+    wv->ctas = 0;
+    /* take everything pending up to the next deep request */
+    size_t first = s->next_pending, last = first;
+    while (last < s->nreqs && !req_is_deep(s, &s->reqs[last])) last++;
     size_t n = last - first;
     pb_req_t *pr = (pb_req_t *)calloc(n, sizeof(*pr));
     if (!pr) return 0;
@@ -310,11 +448,11 @@ static int admit(pose_b200_server_t *s)
 static int reap(pose_b200_server_t *s)
 {
     int k = 0;
-    for (uint32_t i = 0; i < s->max_waves; i++) {
+    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
         wave_t *wv = &s->waves[i];
         if (!wv->busy) continue;
         double t = now_ms();
-        for (size_t r = 0; r < wv->nreqs; r++) {
+        for (size_t r = 0; r < wv->nreqs && !wv->deep; r++) {
             sreq_t *q = &s->reqs[wv->reqs[r]];
             if (q->state == 1 && ((volatile unsigned int *)wv->h_done)[r] >= wv->need[r]) {
                 q->state = 2;
@@ -337,6 +475,7 @@ static int reap(pose_b200_server_t *s)
             cudaGetLastError();
         }
         arena_give(s, wv->arena_off, wv->arena_len);
+        if (wv->deep) s->deep_ctas -= wv->ctas;
         wv->busy = 0;
         k++;
     }
@@ -351,13 +490,13 @@ static void *dispatcher(void *arg)
     pthread_mutex_lock(&s->mu);
     for (;;) {
         int busy = 0;
-        for (uint32_t i = 0; i < s->max_waves; i++) busy |= s->waves[i].busy;
+        for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) busy |= s->waves[i].busy;
         if (!s->running && !busy && s->next_pending >= s->nreqs) break;
         int progress = reap(s);
         while (admit(s)) progress = 1;
         if (!progress) {
             busy = 0;
-            for (uint32_t i = 0; i < s->max_waves; i++) busy |= s->waves[i].busy;
+            for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) busy |= s->waves[i].busy;
             struct timespec ts;
             clock_gettime(CLOCK_REALTIME, &ts);
             long ns = busy ? 50000 : 2000000; /* poll running waves every 50 us */
@@ -396,7 +535,7 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
     s->free_off[0] = 0;
     s->free_len[0] = scratch_bytes;
     s->nfree = 1;
-    for (uint32_t i = 0; i < s->max_waves; i++) {
+    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
         if (cudaStreamCreateWithFlags(&s->waves[i].stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&s->waves[i].done, cudaEventDisableTiming) != cudaSuccess)
             goto fail;
@@ -407,7 +546,7 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
     return s;
 fail:
     cudaGetLastError();
-    for (uint32_t i = 0; i < s->max_waves; i++) {
+    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
         if (s->waves[i].stream) cudaStreamDestroy(s->waves[i].stream);
         if (s->waves[i].done) cudaEventDestroy(s->waves[i].done);
     }
@@ -431,7 +570,7 @@ int pose_b200_server_session(pose_b200_server_t *s, const uint8_t *seed, size_t 
     if (s->sess_bytes + seed_len > s->sess_cap) {
         for (;;) {
             int busy = 0;
-            for (uint32_t i = 0; i < s->max_waves; i++) busy |= s->waves[i].busy;
+            for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) busy |= s->waves[i].busy;
             if (!busy && s->next_pending >= s->nreqs) break;
             pthread_cond_wait(&s->cv, &s->mu);
         }
@@ -557,7 +696,7 @@ void pose_b200_server_destroy(pose_b200_server_t *s)
     pthread_cond_broadcast(&s->cv);
     pthread_mutex_unlock(&s->mu);
     pthread_join(s->thread, NULL);
-    for (uint32_t i = 0; i < s->max_waves; i++) {
+    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
         cudaStreamSynchronize(s->waves[i].stream);
         cudaStreamDestroy(s->waves[i].stream);
         cudaEventDestroy(s->waves[i].done);

@@ -24,7 +24,7 @@ def test_plain_2e17_every_super_chunk(pkg, cuda, wl):
     cb, n = c["chunk_blocks"], c["chunks"]
     buf = cuda.zeros(n * cb * 32, dtype=cuda.uint8, device="cuda")
     with pkg.Topology(cb) as topo:
-        for kernel in (3, 2, 1):
+        for kernel in (3, 1):
             rc, st = topo.label(c["key"], buf.data_ptr(), n * cb * 32, c["rbo"],
                                 sched=pkg.Sched(kernel=kernel), stats=True)
             assert rc == 0, pkg.last_error()

@@ -79,19 +79,6 @@ def test_every_schedule_gives_the_same_bytes(pkg, cuda, wl, T, G):
     assert hashlib.sha256(got).hexdigest() == g["region_sha256"]
 
 
-@pytest.mark.parametrize("T,G", [(4, 1), (8, 1), (16, 1), (4, 2), (8, 2), (16, 2)])
-def test_pipelined_kernel_gives_the_same_bytes(pkg, cuda, wl, oracle, T, G):
-    g = golden("configs.json")["plain_small"]
-    c = wl.plain_small()
-    s = pkg.Sched(team_warps=T, units_per_team=G, kernel=2)
-    got = label_region(pkg, cuda, c["key"], c["chunk_blocks"], c["chunks"], c["rbo"], sched=s)
-    assert hashlib.sha256(got).hexdigest() == g["region_sha256"]
-    for r in golden("small_regions.json"):
-        got = label_region(pkg, cuda, bytes.fromhex(r["key"]), r["chunk_blocks"], r["super_chunks"],
-                           r["rbo"], sched=s)
-        assert got.hex() == r["hex"], (r["chunk_blocks"], r["rbo"])
-
-
 @pytest.mark.parametrize("nc", [7, 15])
 def test_warp_specialised_kernel_gives_the_same_bytes(pkg, cuda, wl, oracle, nc):
     g = golden("configs.json")["plain_small"]
@@ -112,13 +99,11 @@ def test_warp_specialised_kernel_gives_the_same_bytes(pkg, cuda, wl, oracle, nc)
         assert got == oracle.label_region(key, cb, 5, cb * 3, threads=8).tobytes(), cb
 
 
-def test_pipelined_kernel_with_few_teams(pkg, cuda, oracle):
-    rnd = random.Random(5)
-    for cb in (4096, 3000, 37):
-        key = rnd.randbytes(32)
-        s = pkg.Sched(team_warps=4, units_per_team=1, kernel=2, max_teams=3)
-        got = label_region(pkg, cuda, key, cb, 5, cb * 11, sched=s)
-        assert got == oracle.label_region(key, cb, 5, cb * 11, threads=8).tobytes(), cb
+def test_retired_kernel_number_is_refused(pkg, cuda):
+    with pkg.Topology(1024) as topo:
+        buf = cuda.zeros(1024 * 32, dtype=cuda.uint8, device="cuda")
+        assert topo.label(bytes(32), buf.data_ptr(), 1024 * 32, 0, sched=pkg.Sched(kernel=2)) == -1
+        assert "kernel 2" in pkg.last_error()
 
 
 def test_autotune_keeps_the_bytes_and_its_schedule(pkg, cuda, wl):

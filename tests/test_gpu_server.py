@@ -64,3 +64,36 @@ def test_oversized_request_is_rejected(pkg, cuda):
         buf = cuda.zeros(4096 * 32, dtype=cuda.uint8, device="cuda")
         assert srv.submit(topo, sid, buf.data_ptr(), 4096 * 32, 0) == -1  # one copy needs 128 KiB
         assert srv.submit(topo, 99, buf.data_ptr(), 4096 * 32, 0) == -1  # unknown session
+
+
+def test_deep_requests_run_on_the_depth_kernel_and_match_alone(pkg, cuda):
+    """Requests at chunk_blocks 2^17 run alone on the depth kernel while
+    shallow requests keep forming waves around them; every result equals
+    labelling that request alone."""
+    rnd = random.Random(17)
+    deep_cb, cbs = 1 << 17, [1024, 1 << 14]
+    topos = {cb: pkg.Topology(cb) for cb in [deep_cb] + cbs}
+    try:
+        seed_list = [rnd.randbytes(32) for _ in range(3)]
+        plan = [(deep_cb, 2), (1024, 3), (1 << 14, 2), (deep_cb, 3), (1024, 5), (1 << 14, 1), (1024, 2)]
+        reqs = []
+        for cb, ns in plan:
+            reqs.append((cb, ns, cb * rnd.randrange(1 << 16), rnd.randrange(3),
+                         cuda.full((ns * cb * 32,), 0x5A, dtype=cuda.uint8, device="cuda")))
+        cuda.cuda.synchronize()
+        with pkg.Server(scratch_bytes=2 << 30, max_waves=2) as srv:
+            sessions = [srv.session(k) for k in seed_list]
+            tickets = [srv.submit(topos[cb], sessions[sid], buf.data_ptr(), ns * cb * 32, rbo)
+                       for cb, ns, rbo, sid, buf in reqs]
+            assert all(t >= 0 for t in tickets)
+            for t in tickets:
+                rc, q, tot = srv.wait(t)
+                assert rc == 0 and tot >= q >= 0
+        for cb, ns, rbo, sid, buf in reqs:
+            alone = cuda.zeros(ns * cb * 32, dtype=cuda.uint8, device="cuda")
+            assert topos[cb].label(seed_list[sid], alone.data_ptr(), ns * cb * 32, rbo) == 0
+            cuda.cuda.synchronize()
+            assert cuda.equal(alone, buf), (cb, ns, rbo, sid)
+    finally:
+        for t in topos.values():
+            t.free()
