@@ -156,6 +156,15 @@ def profiled_traffic(workload_name: str, kernel: int) -> float | None:
     return None
 
 
+def measured_hbm_gbs() -> float | None:
+    """The pool's measured HBM copy bandwidth (MEASURED_PEAKS.json, written
+    per GPU pod), or None when the file is absent."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return None
+
+
 # ── reference CPU leg ───────────────────────────────────────────────────────
 
 def cpu_reference(w: dict, steps: int, warmup: int, cores: int | None = None) -> dict:
@@ -409,6 +418,8 @@ def run_served(pkg, torch, requests: int = 300, alone: bool = False, rate: float
     lat = [0.0] * len(trace)
     with pkg.Server(scratch_bytes=32 << 30) as srv:  # the library's default wave count
         sid = {s: srv.session(k) for s, k in keys.items()}
+        for t in topos.values():  # set-up, before the trace: the depth kernel's records
+            srv.prepare(t)
         tickets = [None] * len(trace)
         t0 = time.perf_counter()
 
@@ -548,6 +559,7 @@ def run_b200(args) -> None:
     info = topo.info()
     levels = info["levels"]
     traffic = profiled_traffic(w["name"], st0["kernel"]) if not args.chunks else None
+    hbm_gbs = measured_hbm_gbs()
     clocks = clk.summary()
     # depth bound: one label per level on the critical path, each ~comps
     # dependent compressions at the measured compression latency
@@ -570,6 +582,9 @@ def run_b200(args) -> None:
                      "traffic_source": "profiles/: ncu dram__bytes_read.sum + dram__bytes_write.sum per launch"
                                        if traffic is not None else None,
                      "dram_gbs": traffic / (kernel_ms * 1e-3) / 1e9 if traffic is not None else None,
+                     "hbm_peak_gbs": hbm_gbs,
+                     "dram_frac_of_hbm_peak": traffic / (kernel_ms * 1e-3) / 1e9 / hbm_gbs
+                     if traffic is not None and hbm_gbs else None,
                      "peak_source": "measured in this run: k_compress_bench (every SM full, register-resident compressions)",
                      "ops_per_node": comps * ops_per_compress,
                      "spec_ops_per_node": 3 * ops_per_compress,

@@ -31,6 +31,8 @@ typedef struct {
                                    in percent; POSE_B200_PACK_CHAIN packs units while their chain
                                    stays within the launch's longest; 0 = automatic */
     uint32_t flags;             /* POSE_B200_BATCH_* (batched launches); 0 otherwise */
+    uint32_t cluster_ctas;      /* depth kernel: CTAs per chunk copy, a thread-block cluster that
+                                   shares the copy's wide levels (1 = none, 2..16); 0 = automatic */
 } pose_b200_sched_t;
 
 #define POSE_B200_PACK_CHAIN 255u
@@ -51,6 +53,7 @@ typedef struct {
     uint32_t used_cv0_table;    /* 1 when block 0 came from the precomputed table */
     uint32_t kernel;            /* 1 = basic lockstep kernel, 3 = warp-specialised depth kernel,
                                    4 = multi-topology batch kernel */
+    uint32_t cluster_ctas;      /* depth kernel: CTAs per chunk copy (1 = no cluster) */
 } pose_b200_stats_t;
 
 /* Extends pose_graph_hbm_topo_build (common/include/gpu_label.h:77-78).
@@ -182,13 +185,21 @@ int pose_b200_label_stream(const pose_hbm_topo_t *topo, const uint8_t *session_s
  * A labeling service for many concurrent requests.  Session seeds are kept in
  * device memory; requests (the arguments of pose_graph_hbm_topo_label, with a
  * session instead of a seed) can be submitted from any thread at any time.  A
- * dispatcher thread admits the oldest pending requests into a wave — one
- * persistent multi-topology launch on its own stream — whenever a wave slot
- * is free and the scratch arena (the HBM budget given at creation) has room,
- * so work that arrives while other waves run starts as memory frees up and
- * overlaps them on the device.  Each result is byte-identical to labelling
- * the request alone.  All topologies and buffers must be on the device that
- * was current at creation. */
+ * dispatcher thread admits pending requests whenever a slot is free and the
+ * scratch arena (the HBM budget given at creation) has room, so work that
+ * arrives while other work runs starts as memory frees up and overlaps it on
+ * the device:
+ *   - requests of deep topologies (chunk_blocks 2^17 and up) run on the
+ *     multi-unit depth kernel, the pending ones of one topology together,
+ *     1 to 4 chunk copies per CTA as the free SMs allow, at most one such
+ *     CTA per SM, on high-priority streams;
+ *   - the others run in waves: one persistent multi-topology launch per
+ *     wave on its own stream, a request completing as soon as its chunk
+ *     copies are in;
+ *   - a request that waits for SMs or scratch never holds back the others.
+ * Each result is byte-identical to labelling the request alone.  All
+ * topologies and buffers must be on the device that was current at
+ * creation. */
 typedef struct pose_b200_server pose_b200_server_t;
 
 /* scratch_bytes: HBM arena for all waves (0 = half the free memory);
@@ -196,6 +207,11 @@ typedef struct pose_b200_server pose_b200_server_t;
 pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max_waves);
 /* Register a session seed (<= 1016 bytes); returns its id, or -1. */
 int pose_b200_server_session(pose_b200_server_t *server, const uint8_t *seed, size_t seed_len);
+/* Build ahead of the first request what requests of this topology need (the
+ * depth kernel's 512-slot records, for a deep topology; kept with the
+ * topology).  Optional: the first submit of a topology does it otherwise, in
+ * the submitting thread.  0 on success, -1 on a bad argument. */
+int pose_b200_server_prepare(pose_b200_server_t *server, const pose_hbm_topo_t *topo);
 /* Queue one request; returns its ticket, or -1. */
 int64_t pose_b200_server_submit(pose_b200_server_t *server, const pose_hbm_topo_t *topo, int session,
                                 void *hbm_dev_ptr, size_t hbm_len, uint64_t region_block_offset);

@@ -38,7 +38,7 @@ class Sched(C.Structure):
     _fields_ = [("team_warps", C.c_uint32), ("units_per_team", C.c_uint32),
                 ("max_teams", C.c_uint32), ("kernel", C.c_uint32),
                 ("scratch_cap_bytes", C.c_uint64), ("lane_efficiency", C.c_uint32),
-                ("flags", C.c_uint32)]
+                ("flags", C.c_uint32), ("cluster_ctas", C.c_uint32)]
 
 
 PACK_CHAIN = 255  # POSE_B200_PACK_CHAIN: pack units while their chain stays within the launch's longest
@@ -53,7 +53,7 @@ class Stats(C.Structure):
                 ("scratch_bytes", C.c_uint64), ("team_warps", C.c_uint32),
                 ("units_per_team", C.c_uint32), ("teams", C.c_uint32),
                 ("kernel_launches", C.c_uint32), ("used_cv0_table", C.c_uint32),
-                ("kernel", C.c_uint32)]
+                ("kernel", C.c_uint32), ("cluster_ctas", C.c_uint32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -137,6 +137,8 @@ def _declare(L: C.CDLL) -> None:
     L.pose_b200_server_session.restype = C.c_int
     L.pose_b200_server_submit.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_uint64]
     L.pose_b200_server_submit.restype = C.c_int64
+    L.pose_b200_server_prepare.argtypes = [C.c_void_p, C.c_void_p]
+    L.pose_b200_server_prepare.restype = C.c_int
     L.pose_b200_server_wait.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.pose_b200_server_wait.restype = C.c_int
     L.pose_b200_server_query.argtypes = [C.c_void_p, C.c_int64]
@@ -414,6 +416,12 @@ class Server:
         if sid < 0:
             raise RuntimeError("session registration failed")
         return sid
+
+    def prepare(self, topo: "Topology") -> None:
+        """Build what requests of this topology need before the first one
+        arrives (the depth kernel's records of a deep topology)."""
+        if load().pose_b200_server_prepare(self.handle, topo.handle) != 0:
+            raise RuntimeError("server prepare failed")
 
     def submit(self, topo: "Topology", session: int, dev_ptr: int, nbytes: int, rbo: int = 0) -> int:
         return load().pose_b200_server_submit(self.handle, topo.handle, session, C.c_void_p(dev_ptr), nbytes, rbo)

@@ -126,6 +126,12 @@ typedef struct {
     uint32_t team_warps;
     uint32_t nbatches;
     unsigned int *queue;
+    /* k_label_wsc only: CTAs per chunk copy (a cluster), levels wider than
+     * split_width shared by them, and the indices of those levels */
+    uint32_t cluster;
+    uint32_t split_width;
+    const uint32_t *split_levels;
+    uint32_t nsplit;
 } pb_pipe_params_t;
 
 /* Warp-specialised depth-regime kernel (label_ws.cu): team_warps hashing
@@ -133,11 +139,16 @@ typedef struct {
 int pb_dev_label_ws(const pb_pipe_params_t *params, uint32_t grid, uint32_t cta_threads,
                     uint32_t smem_bytes, cudaStream_t stream);
 int pb_dev_label_ws_occupancy(uint32_t cta_threads, uint32_t smem_bytes, int *blocks_per_sm);
+/* The depth kernel with a cluster of params->cluster CTAs per chunk copy
+ * (label_ws.cu, k_label_wsc): params->nunits * cluster CTAs, one copy per
+ * cluster, no work queue. */
+int pb_dev_label_wsc(const pb_pipe_params_t *params, uint32_t smem_bytes, cudaStream_t stream);
+int pb_dev_label_wsc_max_clusters(uint32_t C, uint32_t team_warps, uint32_t smem_bytes, int *clusters);
 
-/* Multi-unit depth kernel (label_ws.cu): k_label_ws with up to 2^g_log2
- * units of one topology per CTA in lockstep.  Batch b is units
- * [b << g_log2, min(nunits, (b + 1) << g_log2)) of `units`; unit k's global
- * label pool is scratch + (cta * G + k % G) * unit_scratch_bytes.  The
+/* Multi-unit depth kernel (label_ws.cu): k_label_ws with G = units_per_cta
+ * (1 to 4) units of one topology per CTA in lockstep.  Batch b is units
+ * [b * G, min(nunits, (b + 1) * G)) of `units`; unit k's global label pool
+ * is scratch + (cta * G + k % G) * unit_scratch_bytes.  The
  * topology's pipelined records are built for a pool of topo.csm slots per
  * unit, and shared memory holds G such pools (pb_wsg_smem_bytes). */
 typedef struct {
@@ -147,13 +158,13 @@ typedef struct {
     uint8_t *scratch;
     uint64_t unit_scratch_bytes; /* topo.gpool * 32 */
     uint32_t nunits;
-    uint32_t g_log2;             /* 0, 1 or 2 */
+    uint32_t units_per_cta;      /* G: 1 to 4 */
     uint32_t team_warps;         /* hashing warps: 7 or 15 */
     uint32_t nbatches;           /* ceil(nunits / G) */
     unsigned int *queue;         /* zeroed work counter */
 } pb_wsg_params_t;
 
-uint32_t pb_wsg_smem_bytes(uint32_t csm, uint32_t g_log2, uint32_t team_warps);
+uint32_t pb_wsg_smem_bytes(uint32_t csm, uint32_t units_per_cta, uint32_t team_warps);
 int pb_dev_label_wsg(const pb_wsg_params_t *params, uint32_t grid, uint32_t cta_threads, uint32_t smem_bytes,
                      cudaStream_t stream);
 /* Raise k_label_wsg's dynamic shared memory limit to the most a CTA can
@@ -177,9 +188,13 @@ int pb_dev_cv0_table(const void *recs, uint32_t S, uint32_t copies, void *cv0, c
 int pb_dev_chunk_seeds(const uint8_t *d_session_seed, uint32_t seed_len, uint64_t rbo, uint32_t cb,
                        uint32_t nchunks, uint64_t first_super, uint32_t *d_seeds,
                        cudaStream_t stream);
-int pb_dev_label(const pb_label_params_t *params, uint32_t grid, uint32_t cta_threads,
+/* smem_bytes: dynamic shared memory per CTA, 0 = the staging area alone
+ * (PB_PREF_BYTES_PER_THREAD per thread); more caps residency per SM
+ * (pb_dev_label_balance_smem). */
+int pb_dev_label(const pb_label_params_t *params, uint32_t grid, uint32_t cta_threads, uint32_t smem_bytes,
                  cudaStream_t stream);
 int pb_dev_label_occupancy(uint32_t cta_threads, int *blocks_per_sm);
+int pb_dev_label_balance_smem(uint32_t cta_threads, uint32_t per_sm, uint32_t *smem_bytes);
 int pb_dev_label_single(uint32_t *d_out, int is_source, uint64_t node_index, const uint32_t *d_in,
                         int have_p0, int have_p1, cudaStream_t stream);
 int pb_dev_compress_bench(uint32_t grid, uint32_t iters, uint32_t salt, uint32_t *d_sink,

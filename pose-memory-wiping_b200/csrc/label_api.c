@@ -92,6 +92,9 @@ struct pose_hbm_topo {
     pb_topo_view_t view;
     pb_topo_view2_t view2; /* pipelined records (d_recs2 != NULL) */
     int occ_ws[2];         /* warp-specialised kernel CTAs/SM for 7 and 15 hashing warps */
+    /* levels wider than split_width (ascending), shared by a cluster's CTAs */
+    uint32_t *d_split, nsplit, split_width;
+    int occ_wsc[4];        /* clusters of 2, 4, 8, 16 CTAs (15 hashing warps) the device holds */
     /* per-topology workspace, reused across calls (one caller thread at a time) */
     cudaStream_t stream;
     cudaEvent_t ev[4];
@@ -102,7 +105,7 @@ struct pose_hbm_topo {
     uint8_t *d_sess;
     size_t sess_alloc;
     unsigned int *d_queue;
-    int occ256, occ512, sms;
+    int occ_team[5], sms; /* k_label CTAs (one team of 2^i warps each) per SM */
     /* pipelined records for a PB_CSM_MULTI-slot shared pool per unit (the
      * multi-unit depth kernel's), built on first use */
     void *d_recs2s;
@@ -136,12 +139,15 @@ static double model_latency(int cv0)
 
 typedef struct {
     uint32_t T, G, teams, grid, cta, kernel, smem, fma;
+    uint32_t per_sm; /* lockstep kernel: teams per SM to cap residency at (0 = no cap) */
+    uint32_t cluster; /* depth kernel: CTAs per chunk copy (1 = k_label_ws, >1 = k_label_wsc) */
     uint64_t team_scratch, scratch_bytes;
     double cost;
 } plan_t;
 
 #define PB_CSM_LATENCY 2048u /* shared-memory label slots per copy in the pipelined records */
 #define PB_CSM_MULTI 512u    /* the same for the multi-unit depth kernel (four pools per CTA) */
+#define PB_SPLIT_WIDTH 480u  /* levels a depth-kernel cluster shares: wider than one pass of its hashing threads */
 
 static double model_ws_latency(void)
 {
@@ -168,6 +174,30 @@ static int ws_occupancy(pose_hbm_topo_t *t, uint32_t nc)
     return t->occ_ws[i];
 }
 
+/* SM clocks a cluster barrier adds to a level (POSE_B200_CLUSTER_SYNC overrides). */
+static double model_cluster_sync(void)
+{
+    const char *e = getenv("POSE_B200_CLUSTER_SYNC");
+    double v = e ? atof(e) : 0.0;
+    return v > 0 ? v : 1500.0;
+}
+
+/* Clusters of C CTAs of the depth kernel (15 hashing warps) the device holds
+ * at once (0 when C is not 2, 4, 8 or 16, or the kernel cannot run so). */
+static int wsc_clusters(pose_hbm_topo_t *t, uint32_t C)
+{
+    const int i = C == 2 ? 0 : C == 4 ? 1 : C == 8 ? 2 : C == 16 ? 3 : -1;
+    if (i < 0 || !t->d_split) return 0;
+    if (t->occ_wsc[i] < 0) {
+        int n = 0;
+        const uint32_t smem = ws_smem_bytes(t, 15);
+        if (smem > 227u * 1024u || pb_dev_label_wsc_max_clusters(C, 15, smem, &n) != 0) n = 0;
+        cudaGetLastError();
+        t->occ_wsc[i] = n;
+    }
+    return t->occ_wsc[i];
+}
+
 static uint64_t passes_lanes(const pose_hbm_topo_t *t, uint64_t lanes)
 {
     uint64_t passes = 0;
@@ -187,13 +217,23 @@ static uint64_t passes_for(const pose_hbm_topo_t *t, uint32_t T, uint32_t G)
 
 static int is_pow2(uint32_t v) { return v && !(v & (v - 1)); }
 
+/* One-warp passes of a batch of G units: sum over levels of ceil(G w / 32).
+ * Warps without a node of a level skip it, so this is the batch's ALU work
+ * in warp-wide node hashes, idle lanes of partly filled warps included. */
+static uint64_t warp_passes(const pose_hbm_topo_t *t, uint32_t G)
+{
+    uint64_t passes = 0;
+    for (uint32_t k = 0; k < t->nw; k++) passes += t->wcnt[k] * (((uint64_t)G * t->wval[k] + 31) / 32);
+    return passes;
+}
+
 /* Throughput model of one launch.  A team's batch takes at least its
  * latency-bound time (every pass of every level waits for a label: t_lat per
  * pass for the basic kernel; the depth kernel's levels cost its per-level
- * time, further passes of a wide level t_lat), and an SM needs at least its ALU time
- * (all node hashes of the teams resident on it at lanes_clk lane-operations
- * per clock).  A launch runs ceil(batches / resident teams) waves of the
- * larger of the two. */
+ * time, further passes of a wide level t_lat), and an SM needs at least its
+ * ALU time (the warp passes of the teams resident on it, 32 lanes each, at
+ * lanes_clk lane-operations per clock).  A launch runs its full waves of the
+ * larger of the two, then the rest of the batches spread over the SMs. */
 static int make_plan(const pose_hbm_topo_t *ct, uint64_t nunits, const pose_b200_sched_t *hint,
                      uint64_t budget, plan_t *best)
 {
@@ -206,49 +246,96 @@ static int make_plan(const pose_hbm_topo_t *ct, uint64_t nunits, const pose_b200
     best->cost = -1;
     for (int kernel = 1; kernel <= 1; kernel++) {
         if (want && want != kernel) continue;
-        for (uint32_t T = 1; T <= 16; T <<= 1) {
+        /* One team per CTA (its barrier is the CTA's, so a CTA reserves one
+         * hardware barrier and the SM's barriers never cap residency), so
+         * that any number k of teams per SM can be resident.  Teams pull
+         * batches until the queue is empty, and a batch's time is set by
+         * the ALU share of its SM.  Every k is costed; a k below the
+         * occupancy limit is enforced by padding the CTA's shared memory
+         * (pb_dev_label_balance_smem), so that no SM takes k + 1. */
+        const char *fk = getenv("POSE_B200_TEAMS_PER_SM"); /* forces k (tests, sweeps) */
+        const int force_k = fk ? atoi(fk) : 0;
+        for (uint32_t T = 1, ti = 0; T <= 16; T <<= 1, ti++) {
             if (hint && hint->team_warps && hint->team_warps != T) continue;
-            uint32_t cta = T == 16 ? 512 : 256;
-            uint32_t tpc = cta / (32 * T);
+            const uint32_t cta = 32 * T;
+            const int occ = t->occ_team[ti];
+            if (occ <= 0) continue;
             for (uint32_t G = 1; G <= 32 && G <= 32 * T; G <<= 1) {
                 if (hint && hint->units_per_team && hint->units_per_team != G) continue;
-                int occ = T == 16 ? t->occ512 : t->occ256;
-                if (occ <= 0) continue;
                 uint64_t slots = t->pool;
                 uint64_t team_scratch = (uint64_t)G * slots * 32;
                 uint64_t batches = (nunits + G - 1) / G;
-                uint64_t cap = (uint64_t)t->sms * occ * tpc;
                 uint64_t memcap = budget / team_scratch;
-                uint64_t R = cap < memcap ? cap : memcap;
-                if (R > batches) R = batches;
-                if (hint && hint->max_teams && R > hint->max_teams) R = hint->max_teams;
-                if (R == 0) continue;
-                if (R > tpc && R < batches) R -= R % tpc; /* whole CTAs when capped */
-                uint64_t grid = (R + tpc - 1) / tpc;
-                uint64_t sbytes = grid * tpc * team_scratch;
-                if (sbytes > budget) continue;
-                uint64_t waves = (batches + R - 1) / R;
                 uint64_t passes = passes_for(t, T, G);
                 double lat = (double)passes * t_lat;
-                double teams_sm = (double)((R + t->sms - 1) / t->sms);
-                double alu = teams_sm * G * (double)t->S * item_instr / lanes_clk;
-                double cost = (double)waves * (lat > alu ? lat : alu);
-                if (best->cost < 0 || cost < best->cost * 0.999 ||
-                    (cost <= best->cost * 1.001 && sbytes < best->scratch_bytes)) {
-                    best->T = T; best->G = G; best->teams = (uint32_t)R;
-                    best->grid = (uint32_t)grid; best->cta = cta;
-                    best->team_scratch = team_scratch; best->scratch_bytes = sbytes;
-                    best->cost = cost; best->kernel = (uint32_t)kernel;
-                    best->smem = 0;
-                    best->fma = kernel == 1 && alu >= lat; /* ALU-bound: move adds to the FMA pipe */
+                /* one batch's ALU clocks on an SM of its own: its warp passes
+                 * of 32 lanes, idle lanes included */
+                const double alu1 = (double)warp_passes(t, G) * 32.0 * item_instr / lanes_clk;
+                for (int k = occ; k >= 1; k--) {
+                    if (force_k && k != force_k) continue;
+                    uint64_t R = (uint64_t)t->sms * (uint64_t)k;
+                    if (R > memcap) R = memcap;
+                    if (R > batches) R = batches;
+                    if (hint && hint->max_teams && R > hint->max_teams) R = hint->max_teams;
+                    if (R == 0) continue;
+                    uint64_t sbytes = R * team_scratch;
+                    if (sbytes > budget) continue;
+                    /* full waves of R teams, then the rest, spread over the SMs */
+                    const uint64_t full = batches / R, rest = batches - full * R;
+                    const uint64_t teams_sm = (R + t->sms - 1) / t->sms, rest_sm = (rest + t->sms - 1) / t->sms;
+                    const double alu = (double)teams_sm * alu1, alu_rest = (double)rest_sm * alu1;
+                    double cost = (double)full * (lat > alu ? lat : alu);
+                    if (rest) cost += lat > alu_rest ? lat : alu_rest;
+                    if (best->cost < 0 || cost < best->cost * 0.999 ||
+                        (cost <= best->cost * 1.001 && sbytes < best->scratch_bytes)) {
+                        best->T = T; best->G = G; best->teams = (uint32_t)R;
+                        best->grid = (uint32_t)R; best->cta = cta;
+                        best->team_scratch = team_scratch; best->scratch_bytes = sbytes;
+                        best->cost = cost; best->kernel = (uint32_t)kernel;
+                        /* residency cap when fewer than the occupancy limit
+                         * of teams go on every SM */
+                        best->smem = 0;
+                        best->per_sm = R % t->sms == 0 && R / t->sms < (uint64_t)occ ? (uint32_t)(R / t->sms) : 0;
+                        best->fma = kernel == 1 && alu >= lat; /* ALU-bound: move adds to the FMA pipe */
+                    }
                 }
             }
+        }
+    }
+    /* warp-specialised kernel with a cluster of C CTAs per chunk copy: one
+     * wave of nunits clusters, the levels wider than split_width shared by
+     * the cluster (their extra passes divided by C, two cluster barriers
+     * each at most) */
+    for (uint32_t C = 2; C <= 16 && t->d_split && (!want || want == 3); C <<= 1) {
+        const uint32_t nc = 15;
+        if (hint && hint->team_warps && hint->team_warps != nc) continue;
+        if (hint && hint->units_per_team > 1) continue;
+        if (hint && hint->cluster_ctas && hint->cluster_ctas != C) continue;
+        if (!(hint && hint->cluster_ctas == C) && C > 8) continue; /* 16 only on request */
+        const int ncl = wsc_clusters(t, C);
+        if (ncl <= 0 || nunits > (uint64_t)ncl) continue;
+        if (hint && hint->max_teams && nunits > hint->max_teams) continue;
+        uint64_t team_scratch = (uint64_t)(t->view2.gpool ? t->view2.gpool : 1) * 32;
+        uint64_t sbytes = nunits * team_scratch;
+        if (sbytes > budget) continue;
+        uint64_t passes = passes_lanes(t, 32ull * nc);
+        double lat = (double)t->L * model_ws_latency() + (double)(passes - t->L) * t_lat / C +
+                     2.0 * t->nsplit * model_cluster_sync();
+        double cost = lat;
+        if (best->cost < 0 || cost < best->cost * 0.999) {
+            best->T = nc; best->G = 1; best->teams = (uint32_t)nunits;
+            best->grid = (uint32_t)(nunits * C); best->cta = 32 * (nc + 1);
+            best->team_scratch = team_scratch; best->scratch_bytes = sbytes;
+            best->cost = cost; best->kernel = 3; best->smem = ws_smem_bytes(t, nc); best->fma = 0;
+            best->per_sm = 0;
+            best->cluster = C;
         }
     }
     /* warp-specialised kernel: one chunk copy per CTA, NC hashing warps */
     for (uint32_t nc = 7; nc <= 15 && t->d_recs2 && (!want || want == 3); nc += 8) {
         if (hint && hint->team_warps && hint->team_warps != nc) continue;
         if (hint && hint->units_per_team > 1) continue;
+        if (hint && hint->cluster_ctas > 1) continue;
         int occ = ws_occupancy(t, nc);
         if (occ <= 0) continue;
         uint64_t team_scratch = (uint64_t)(t->view2.gpool ? t->view2.gpool : 1) * 32;
@@ -272,6 +359,8 @@ static int make_plan(const pose_hbm_topo_t *ct, uint64_t nunits, const pose_b200
             best->grid = (uint32_t)R; best->cta = 32 * (nc + 1);
             best->team_scratch = team_scratch; best->scratch_bytes = sbytes;
             best->cost = cost; best->kernel = 3; best->smem = ws_smem_bytes(t, nc); best->fma = 0;
+            best->per_sm = 0;
+            best->cluster = 1;
         }
     }
     return best->cost < 0 ? -1 : 0;
@@ -363,6 +452,7 @@ void pose_graph_hbm_topo_free(pose_hbm_topo_t *t)
     cudaFree(t->d_recs);
     cudaFree(t->d_recs2);
     cudaFree(t->d_recs2s);
+    cudaFree(t->d_split);
     cudaFree(t->d_cv0);
     cudaFree(t->d_orank);
     cudaFree(t->d_lstart);
@@ -460,10 +550,11 @@ static pose_hbm_topo_t *pose_b200_topo_build_impl(uint32_t chunk_blocks, int wit
             }
         }
         CK(cudaStreamSynchronize(t->stream), "build");
-        if (pb_dev_label_occupancy(256, &t->occ256) != 0 || pb_dev_label_occupancy(512, &t->occ512) != 0) {
-            set_err("pose_graph_hbm_topo_build: occupancy query failed");
-            goto fail;
-        }
+        for (int i = 0; i < 5; i++)
+            if (pb_dev_label_occupancy(32u << i, &t->occ_team[i]) != 0) {
+                set_err("pose_graph_hbm_topo_build: occupancy query failed");
+                goto fail;
+            }
         CK(cudaDeviceGetAttribute(&t->sms, cudaDevAttrMultiProcessorCount, t->device), "SM count");
         t->view.recs = (const pb_u4 *)t->d_recs;
         t->view.cv0 = (const pb_u4 *)t->d_cv0;
@@ -481,6 +572,29 @@ static pose_hbm_topo_t *pose_b200_topo_build_impl(uint32_t chunk_blocks, int wit
         t->view2.retained = h.retained; t->view2.csm = h.csm; t->view2.gpool = h.gpool2;
         memcpy(t->view2.desc, t->view.desc, sizeof(t->view2.desc));
         memset(t->occ_ws, 0xFF, sizeof(t->occ_ws));
+        memset(t->occ_wsc, 0xFF, sizeof(t->occ_wsc));
+        if (t->d_recs2) {
+            /* the levels a cluster of the depth kernel shares: wider than
+             * split_width (POSE_B200_SPLIT_WIDTH overrides the default, the
+             * depth kernel's hashing threads) */
+            const char *e = getenv("POSE_B200_SPLIT_WIDTH");
+            t->split_width = e && e[0] ? (uint32_t)strtoul(e, NULL, 10) : PB_SPLIT_WIDTH;
+            uint32_t n = 0;
+            for (uint32_t l = 0; l < h.L; l++) n += h.lstart[l + 1] - h.lstart[l] > t->split_width;
+            if (n) {
+                uint32_t *hs = (uint32_t *)malloc((size_t)n * 4);
+                if (!hs) { set_err("pose_graph_hbm_topo_build: out of host memory"); goto fail; }
+                n = 0;
+                for (uint32_t l = 0; l < h.L; l++)
+                    if (h.lstart[l + 1] - h.lstart[l] > t->split_width) hs[n++] = l;
+                cudaError_t e1 = pb_dev_malloc((void **)&t->d_split, (size_t)n * 4);
+                if (e1 == cudaSuccess) e1 = cudaMemcpy(t->d_split, hs, (size_t)n * 4, cudaMemcpyHostToDevice);
+                free(hs);
+                CK(e1, "split levels");
+                t->nsplit = n;
+                t->dev_bytes += (uint64_t)n * 4;
+            }
+        }
     }
     pb_topo_host_free(&h);
     return t;
@@ -550,6 +664,7 @@ int pose_b200_plan(const pose_hbm_topo_t *t, uint64_t super_chunks, const pose_b
     out->max_teams = p.teams;
     out->kernel = p.kernel;
     out->scratch_cap_bytes = p.scratch_bytes;
+    out->cluster_ctas = p.kernel == 3 ? p.cluster : 0;
     return 0;
 }
 
@@ -581,13 +696,17 @@ static int autotune_candidates(pose_hbm_topo_t *t, uint64_t nunits, uint64_t bud
             c[n].s.kernel = 1; c[n].s.team_warps = p.T; c[n].s.units_per_team = p.G; c[n].s.max_teams = p.teams;
             c[n].cost = p.cost; c[n].group = T; n++;
         }
-    pose_b200_sched_t h;
-    memset(&h, 0, sizeof(h));
-    h.kernel = 3;
-    plan_t p;
-    if (make_plan(t, nunits, &h, budget, &p) == 0) {
+    /* the depth kernel alone and with a cluster of 2, 4 or 8 CTAs per copy */
+    for (uint32_t cl = 1; cl <= 8 && n < PB_TUNE_MAX; cl <<= 1) {
+        pose_b200_sched_t h;
+        memset(&h, 0, sizeof(h));
+        h.kernel = 3;
+        h.cluster_ctas = cl;
+        plan_t p;
+        if (make_plan(t, nunits, &h, budget, &p) != 0) continue;
         memset(&c[n], 0, sizeof(c[n]));
         c[n].s.kernel = 3; c[n].s.team_warps = p.T; c[n].s.units_per_team = 1; c[n].s.max_teams = p.teams;
+        c[n].s.cluster_ctas = p.cluster;
         c[n].cost = p.cost; c[n].group = 0; n++;
     }
     /* by modelled cost */
@@ -682,6 +801,11 @@ static int topo_label_core_impl(const pose_hbm_topo_t *ct, const uint8_t *sessio
                   (sched->units_per_team &&
                    (!is_pow2(sched->units_per_team) || sched->units_per_team > 32)))) {
         set_err("pose_b200_topo_label: schedule must use powers of two (T <= 16, G <= 32)");
+        return -1;
+    }
+    if (sched && sched->cluster_ctas > 1 &&
+        ((sched->kernel != 0 && sched->kernel != 3) || !is_pow2(sched->cluster_ctas) || sched->cluster_ctas > 16)) {
+        set_err("pose_b200_topo_label: cluster_ctas must be 0, 1, 2, 4, 8 or 16, with the depth kernel");
         return -1;
     }
     if (sched && sched->kernel > 3) {
@@ -804,9 +928,23 @@ static int topo_label_core_impl(const pose_hbm_topo_t *ct, const uint8_t *sessio
                 pp.team_scratch_bytes = plan.team_scratch; pp.nunits = p.nunits;
                 pp.copies_log2 = p.copies_log2; pp.g_log2 = p.g_log2; pp.team_warps = p.team_warps;
                 pp.nbatches = p.nbatches; pp.queue = p.queue;
-                lrc = pb_dev_label_ws(&pp, plan.grid, plan.cta, plan.smem, t->stream);
+                if (plan.cluster > 1) {
+                    pp.cluster = plan.cluster;
+                    pp.split_width = t->split_width;
+                    pp.split_levels = t->d_split;
+                    pp.nsplit = t->nsplit;
+                    lrc = pb_dev_label_wsc(&pp, plan.smem, t->stream);
+                } else {
+                    lrc = pb_dev_label_ws(&pp, plan.grid, plan.cta, plan.smem, t->stream);
+                }
             } else {
-                lrc = pb_dev_label(&p, plan.grid, plan.cta, t->stream);
+                uint32_t smem = 0;
+                const char *pad = getenv("POSE_B200_BALANCE_SMEM");
+                if (plan.per_sm && !(pad && pad[0] == '0') &&
+                    pb_dev_label_balance_smem(plan.cta, plan.per_sm, &smem) != 0)
+                    smem = 0;
+                cudaGetLastError();
+                lrc = pb_dev_label(&p, plan.grid, plan.cta, smem, t->stream);
             }
             if (lrc != 0) {
                 set_err("pose_graph_hbm_topo_label: label kernel launch failed: %s",
@@ -844,6 +982,7 @@ static int topo_label_core_impl(const pose_hbm_topo_t *ct, const uint8_t *sessio
             stats->kernel_launches = launches;
             stats->used_cv0_table = t->d_cv0 != NULL;
             stats->kernel = plan.kernel;
+            stats->cluster_ctas = plan.kernel == 3 ? (plan.cluster ? plan.cluster : 1) : 0;
         }
         if (!quiet() && elapsed > 0) {
             double mib = (double)(num_super * t->super_bytes) / (double)(1u << 20);
@@ -1091,36 +1230,6 @@ int pb_topo_internal(const pose_hbm_topo_t *t, pb_topo_internal_t *out)
     out->stream = t->stream;
     out->sms = t->sms;
     return 0;
-}
-
-uint64_t pb_topo_depth_unit_scratch(const pose_hbm_topo_t *t)
-{
-    return t && t->d_recs2 && t->d_cv0 ? (uint64_t)(t->view2.gpool ? t->view2.gpool : 1) * 32 : 0;
-}
-
-int pb_topo_launch_depth(const pose_hbm_topo_t *ct, const uint32_t *d_seeds, void *dev_ptr, uint64_t nsuper,
-                         uint8_t *scratch, uint32_t grid, unsigned int *d_queue, cudaStream_t stream)
-{
-    pose_hbm_topo_t *t = (pose_hbm_topo_t *)ct; /* occupancy cache */
-    const uint32_t nc = 15;
-    if (!pb_topo_depth_unit_scratch(t) || nsuper == 0 || grid == 0 || nsuper * t->copies > 0xFFFFFFFFull) return -1;
-    if (ws_occupancy(t, nc) <= 0) return -1;
-    pb_pipe_params_t pp;
-    memset(&pp, 0, sizeof(pp));
-    pp.topo = t->view2;
-    pp.seeds = d_seeds;
-    pp.persist = (uint8_t *)dev_ptr;
-    pp.super_bytes = t->super_bytes;
-    pp.first_super = 0;
-    pp.scratch = scratch;
-    pp.team_scratch_bytes = pb_topo_depth_unit_scratch(t);
-    pp.nunits = (uint32_t)(nsuper * t->copies);
-    pp.copies_log2 = t->copies == 2 ? 1 : 0;
-    pp.g_log2 = 0;
-    pp.team_warps = nc;
-    pp.nbatches = pp.nunits;
-    pp.queue = d_queue;
-    return pb_dev_label_ws(&pp, grid, 32 * (nc + 1), ws_smem_bytes(t, nc), stream);
 }
 
 int pb_topo_view2_small(const pose_hbm_topo_t *ct, pb_topo_view2_t *out)

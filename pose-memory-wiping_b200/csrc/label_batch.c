@@ -35,7 +35,7 @@
 
 /* One launch of a batch: its tables, scratch and queue.  kind 0 runs the
  * lockstep multi-topology kernel, kind 1 the multi-unit depth kernel (one
- * topology; v2, glog and smem describe it). */
+ * topology; v2, units_per_cta and smem describe it). */
 typedef struct {
     void *d_topos, *d_batches, *d_units, *d_jobs, *d_seeds, *d_scratch, *d_queue;
     uint64_t scratch_bytes, nodes, super_chunks, units, nbatches, njobs;
@@ -43,7 +43,7 @@ typedef struct {
     uint64_t team_scratch;
     int kind;
     pb_topo_view2_t v2;
-    uint32_t glog, smem;
+    uint32_t units_per_cta, smem;
 } batch_part_t;
 
 struct pose_b200_batch {
@@ -407,15 +407,15 @@ static int part_setup(pose_b200_batch_t *b, batch_part_t *q, const pb_plan_table
 }
 
 /* The deep part on the multi-unit depth kernel: every unit of pl (one
- * topology, records v2), 2^glog units per CTA, at most one CTA per SM
+ * topology, records v2), G (1 to 4) units per CTA, at most one CTA per SM
  * (`sms` CTAs), 15 hashing warps.  Returns 0, or -1 (message on stderr). */
 static int part_setup_wsg(pose_b200_batch_t *b, batch_part_t *q, const pb_plan_tables_t *pl,
-                          const pb_topo_view2_t *v2, uint32_t glog, uint32_t sms, uint32_t smem)
+                          const pb_topo_view2_t *v2, uint32_t G, uint32_t sms, uint32_t smem)
 {
-    const uint32_t G = 1u << glog, NC = 15;
+    const uint32_t NC = 15;
     q->kind = 1;
     q->v2 = *v2;
-    q->glog = glog;
+    q->units_per_cta = G;
     q->T = NC;
     q->units = pl->nunits;
     q->njobs = pl->njobs;
@@ -432,7 +432,7 @@ static int part_setup_wsg(pose_b200_batch_t *b, batch_part_t *q, const pb_plan_t
     q->team_scratch = (uint64_t)G * v2->gpool * 32;
     q->scratch_bytes = (uint64_t)q->grid * q->team_scratch;
     uint32_t max_smem = 0;
-    if (pb_dev_label_wsg_prepare(&max_smem) != 0 || pb_wsg_smem_bytes(v2->csm, glog, NC) > max_smem) {
+    if (pb_dev_label_wsg_prepare(&max_smem) != 0 || pb_wsg_smem_bytes(v2->csm, G, NC) > max_smem) {
         fprintf(stderr, "pose_b200_batch_create: shared memory attribute: %s\n", cudaGetErrorString(cudaGetLastError()));
         return -1;
     }
@@ -488,7 +488,7 @@ static int part_capture(const pose_b200_batch_t *b, const batch_part_t *q, cudaS
         w.scratch = (uint8_t *)q->d_scratch;
         w.unit_scratch_bytes = (uint64_t)q->v2.gpool * 32;
         w.nunits = (uint32_t)q->units;
-        w.g_log2 = q->glog;
+        w.units_per_cta = q->units_per_cta;
         w.team_warps = q->T;
         w.nbatches = (uint32_t)q->nbatches;
         w.queue = (unsigned int *)q->d_queue;
@@ -596,29 +596,34 @@ no_split:
                 if (pd[i].topo != pd[0].topo) one_topo = 0;
             }
             /* one topology: the multi-unit depth kernel, with the fewest
-             * units per CTA (1, 2 or 4) that fit one CTA per SM */
+             * units per CTA (1, 2 or 4) that fit one CTA per SM: a narrow
+             * level of G units is still one warp pass, while a wide level's
+             * ALU work on the SM grows with G.  (Three units per CTA, 137
+             * CTAs for the 256-session workload's 410 deep units, measured
+             * 2.12 s against 1.62 s for four: the shallow part then has 34
+             * SMs fewer.) */
             pb_topo_view2_t v2;
-            uint32_t glog = 0;
-            while (glog < 2 && ((dunits + (1u << glog) - 1) >> glog) > sms) glog++;
+            uint32_t G = 1;
+            while (G < 4 && (dunits + G - 1) / G > sms) G *= 2;
             const char *ek = getenv("POSE_B200_DEEP_KERNEL");
             const char *eg = getenv("POSE_B200_DEEP_UNITS");
-            if (eg && (eg[0] == '1' || eg[0] == '2' || eg[0] == '4') && !eg[1]) glog = eg[0] == '1' ? 0 : eg[0] == '2' ? 1 : 2;
+            if (eg && eg[0] >= '1' && eg[0] <= '4' && !eg[1]) G = (uint32_t)(eg[0] - '0');
             int wsg = !(ek && ek[0] == '0') && one_topo && pb_topo_view2_small(pd[0].topo, &v2) == 0;
             if (wsg) {
-                const uint64_t grid = ((dunits + (1u << glog) - 1) >> glog) < sms ? ((dunits + (1u << glog) - 1) >> glog) : sms;
-                wsg = grid * ((uint64_t)v2.gpool * 32 << glog) <= budget;
+                const uint64_t grid = (dunits + G - 1) / G < sms ? (dunits + G - 1) / G : sms;
+                wsg = grid * ((uint64_t)v2.gpool * 32 * G) <= budget;
             }
             if (wsg) {
                 /* a device whose CTAs cannot hold the kernel's shared memory
                  * keeps the deep part on the lockstep kernel */
                 uint32_t max_smem = 0;
-                wsg = pb_dev_label_wsg_prepare(&max_smem) == 0 && pb_wsg_smem_bytes(v2.csm, glog, 15) <= max_smem;
+                wsg = pb_dev_label_wsg_prepare(&max_smem) == 0 && pb_wsg_smem_bytes(v2.csm, G, 15) <= max_smem;
                 cudaGetLastError();
             }
             if (wsg) {
-                const uint32_t smem = pb_wsg_smem_bytes(v2.csm, glog, 15);
+                const uint32_t smem = pb_wsg_smem_bytes(v2.csm, G, 15);
                 if (pb_plan_requests(pd, nd, 8, 1, 0.9999, &pl[1]) != 0 || pl[1].nunits == 0) goto fail;
-                if (part_setup_wsg(b, &b->part[1], &pl[1], &v2, glog, sms, smem) != 0) goto fail;
+                if (part_setup_wsg(b, &b->part[1], &pl[1], &v2, G, sms, smem) != 0) goto fail;
             } else {
                 uint32_t g = 1;
                 while (g < 4 && 2 * (dunits + g - 1) / g > (uint64_t)sms * occ) g *= 2;

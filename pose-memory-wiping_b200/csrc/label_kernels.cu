@@ -38,10 +38,17 @@ __constant__ uint32_t c_key_src[8];
 __constant__ uint32_t c_key_int[8];
 __constant__ uint32_t c_key_chunk_seed[8];
 
+/* Team barrier.  CTA_TEAM: the team is the whole CTA, so barrier 0 serves
+ * (a kernel that names only barrier 0 reserves one barrier per CTA, not all
+ * sixteen, and its CTAs are not held back by the SM's barrier count);
+ * otherwise the named barrier bar_id over the team's nthreads threads. */
+template <bool CTA_TEAM>
 __device__ __forceinline__ void team_sync(uint32_t team_warps, uint32_t bar_id, uint32_t nthreads)
 {
     if (team_warps == 1) {
         __syncwarp();
+    } else if (CTA_TEAM) {
+        __syncthreads();
     } else {
         asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
     }
@@ -170,7 +177,7 @@ __device__ __forceinline__ uint4 staged(uint32_t b, uint32_t k)
  * two levels ahead, so that a level's dependent chain is only the
  * predecessor loads, the two compressions and the barrier.  Each thread
  * reads back only its own staging slots, after waiting for its own copies. */
-template <bool FMA>
+template <bool FMA, bool CTA_TEAM>
 __device__ __forceinline__ void label_levels(const pb_topo_view_t &tp, const UnitCtx &c, uint32_t T,
                                              uint32_t bar_id, uint32_t TT, uint32_t one)
 {
@@ -250,7 +257,7 @@ __device__ __forceinline__ void label_levels(const pb_topo_view_t &tp, const Uni
                 }
             }
         }
-        team_sync(T, bar_id, TT);
+        team_sync<CTA_TEAM>(T, bar_id, TT);
         s0 = s1;
         s1 = s2;
         s2 = s3;
@@ -258,6 +265,7 @@ __device__ __forceinline__ void label_levels(const pb_topo_view_t &tp, const Uni
 }
 
 /* Team-wide batch index from the work counter. */
+template <bool CTA_TEAM>
 __device__ __forceinline__ uint32_t grab_batch(unsigned int *queue, uint32_t T, uint32_t team, uint32_t tt,
                                                uint32_t bar_id, uint32_t TT, uint32_t *s_batch)
 {
@@ -267,24 +275,25 @@ __device__ __forceinline__ uint32_t grab_batch(unsigned int *queue, uint32_t T, 
         return __shfl_sync(0xFFFFFFFFu, b, 0);
     }
     if (tt == 0) s_batch[team] = atomicAdd(queue, 1u);
-    team_sync(T, bar_id, TT);
+    team_sync<CTA_TEAM>(T, bar_id, TT);
     const uint32_t b = s_batch[team];
-    team_sync(T, bar_id, TT);
+    team_sync<CTA_TEAM>(T, bar_id, TT);
     return b;
 }
 
+/* The lockstep kernel for one topology: one team of T warps per CTA
+ * (blockDim.x == 32 T), so any number of teams can be resident per SM. */
 template <bool FMA>
 __global__ void __launch_bounds__(PB_CTA_THREADS) k_label(const __grid_constant__ pb_label_params_t p)
 {
     const uint32_t T = p.team_warps;
     const uint32_t TT = T * 32;
-    const uint32_t team = (threadIdx.x >> 5) / T;
-    const uint32_t tt = threadIdx.x - team * TT;
-    const uint32_t teams_per_cta = blockDim.x / TT;
-    const uint64_t gteam = (uint64_t)blockIdx.x * teams_per_cta + team;
-    const uint32_t bar_id = 1 + team;
+    const uint32_t team = 0;
+    const uint32_t tt = threadIdx.x;
+    const uint64_t gteam = blockIdx.x;
+    const uint32_t bar_id = 0;
     const pb_topo_view_t &tp = p.topo;
-    __shared__ uint32_t s_batch[PB_CTA_THREADS / 32];
+    __shared__ uint32_t s_batch[1];
     UnitCtx c;
     c.glog = p.g_log2;
     c.u = tt & ((1u << c.glog) - 1);
@@ -293,7 +302,7 @@ __global__ void __launch_bounds__(PB_CTA_THREADS) k_label(const __grid_constant_
     c.tscr = reinterpret_cast<uint4 *>(p.scratch + gteam * p.team_scratch_bytes);
 
     for (;;) {
-        const uint32_t batch = grab_batch(p.queue, T, team, tt, bar_id, TT, s_batch);
+        const uint32_t batch = grab_batch<true>(p.queue, T, team, tt, bar_id, TT, s_batch);
         if (batch >= p.nbatches) break;
         const uint32_t unit = (batch << c.glog) + c.u;
         c.valid = unit < p.nunits;
@@ -306,7 +315,7 @@ __global__ void __launch_bounds__(PB_CTA_THREADS) k_label(const __grid_constant_
         c.cv0 = tp.cv0 ? tp.cv0 + (uint64_t)copy * tp.S * 2 : nullptr;
 #pragma unroll
         for (int i = 0; i < 8; i++) c.seed[i] = c.valid ? p.seeds[8 * (size_t)chunk + i] : 0u;
-        label_levels<FMA>(tp, c, T, bar_id, TT, p.one);
+        label_levels<FMA, true>(tp, c, T, bar_id, TT, p.one);
     }
 }
 
@@ -329,13 +338,13 @@ __global__ void __launch_bounds__(PB_MULTI_CTA_THREADS, 3) k_label_multi(const _
     c.tscr = reinterpret_cast<uint4 *>(p.scratch + gteam * p.team_scratch_bytes);
 
     for (;;) {
-        const uint32_t batch = grab_batch(p.queue, T, team, tt, bar_id, TT, s_batch);
+        const uint32_t batch = grab_batch<false>(p.queue, T, team, tt, bar_id, TT, s_batch);
         if (batch >= p.nbatches) break;
         const pb_mbatch_t bd = p.batches[batch];
         if (tt < sizeof(pb_topo_view_t) / 4)
             reinterpret_cast<uint32_t *>(&s_topo[team])[tt] =
                 reinterpret_cast<const uint32_t *>(p.topos + bd.topo)[tt];
-        team_sync(T, bar_id, TT);
+        team_sync<false>(T, bar_id, TT);
         const pb_topo_view_t &tp = s_topo[team];
         c.glog = bd.glog;
         c.u = tt & ((1u << c.glog) - 1);
@@ -351,14 +360,14 @@ __global__ void __launch_bounds__(PB_MULTI_CTA_THREADS, 3) k_label_multi(const _
         c.cv0 = tp.cv0 ? tp.cv0 + (uint64_t)copy * tp.S * 2 : nullptr;
 #pragma unroll
         for (int i = 0; i < 8; i++) c.seed[i] = c.valid ? p.seeds[8 * (size_t)un.seed + i] : 0u;
-        label_levels<FMA>(tp, c, T, bar_id, TT, p.one);
+        label_levels<FMA, false>(tp, c, T, bar_id, TT, p.one);
         /* label_levels ended with a team barrier, so every persisted label of
          * the batch is ordered before this fence */
         if (p.req_done != nullptr && tt < bd.count) {
             __threadfence_system();
             atomicAdd_system(p.req_done + p.unit_req[bd.first_unit + tt], 1u);
         }
-        team_sync(T, bar_id, TT); /* s_topo[team] is rewritten by the next batch */
+        team_sync<false>(T, bar_id, TT); /* s_topo[team] is rewritten by the next batch */
     }
 }
 
@@ -528,11 +537,21 @@ static void allow_stage_smem()
 }
 
 extern "C" int pb_dev_label(const pb_label_params_t *params, uint32_t grid, uint32_t cta_threads,
-                            cudaStream_t stream)
+                            uint32_t smem_bytes, cudaStream_t stream)
 {
+    if (cta_threads != 32u * params->team_warps || cta_threads > PB_CTA_THREADS) return -1; /* one team per CTA */
     cudaGetLastError(); /* report only this launch */
-    const uint32_t smem = PB_PREF_BYTES_PER_THREAD * cta_threads;
-    if (smem > 48 * 1024 - 1024) allow_stage_smem();
+    uint32_t smem = PB_PREF_BYTES_PER_THREAD * cta_threads;
+    if (smem_bytes > smem) {
+        if (cudaFuncSetAttribute(pb::k_label<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(pb::k_label<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes) !=
+                cudaSuccess)
+            return -1;
+        smem = smem_bytes;
+    } else if (smem > 48 * 1024 - 1024) {
+        allow_stage_smem();
+    }
     cudaGetLastError();
     if (params->fma_adds) pb::k_label<true><<<grid, cta_threads, smem, stream>>>(*params);
     else pb::k_label<false><<<grid, cta_threads, smem, stream>>>(*params);
@@ -568,6 +587,52 @@ extern "C" int pb_dev_seed_jobs(const void *jobs, uint32_t njobs, const uint8_t 
     cudaGetLastError(); /* report only this launch */
     pb::k_seed_jobs<<<(njobs + 127) / 128, 128, 0, stream>>>((const pb_seedjob_t *)jobs, njobs, blob, seeds);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+/* Dynamic shared memory per CTA of k_label with cta_threads threads that
+ * lets at most `per_sm` such CTAs reside on one SM (the staging area is the
+ * least it gets): *smem_bytes = 0 when the staging area alone already holds
+ * residency to per_sm or below.  A launch of per_sm x SMs CTAs then puts
+ * exactly per_sm teams on every SM, so the waves of a persistent launch end
+ * together on every SM. */
+extern "C" int pb_dev_label_balance_smem(uint32_t cta_threads, uint32_t per_sm, uint32_t *smem_bytes)
+{
+    int dev = 0, cap = 0, resv = 0, optin = 0, occ = 0;
+    *smem_bytes = 0;
+    if (per_sm == 0 || cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        return -1;
+    const uint32_t base = PB_PREF_BYTES_PER_THREAD * cta_threads;
+    if (pb_dev_label_occupancy(cta_threads, &occ) != 0) return -1;
+    if ((uint32_t)occ <= per_sm) return 0;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, pb::k_label<true>) != cudaSuccess) return -1;
+    /* largest multiple of 1 KiB with per_sm CTAs fitting the SM's shared memory */
+    int64_t each = (int64_t)cap / per_sm - resv - (int64_t)fa.sharedSizeBytes;
+    each -= each % 1024;
+    if (each > optin - (int64_t)fa.sharedSizeBytes) each = optin - (int64_t)fa.sharedSizeBytes;
+    if (each < (int64_t)base) return 0;
+    for (; each >= (int64_t)base; each -= 1024) {
+        int a = 0, b = 0;
+        if (cudaFuncSetAttribute(pb::k_label<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)each) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(pb::k_label<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)each) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, pb::k_label<false>, (int)cta_threads, each) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, pb::k_label<true>, (int)cta_threads, each) !=
+                cudaSuccess)
+            return -1;
+        const int m = a > b ? a : b;
+        if ((uint32_t)m == per_sm) {
+            *smem_bytes = (uint32_t)each;
+            return 0;
+        }
+        if ((uint32_t)m > per_sm) break;
+    }
+    return 0;
 }
 
 extern "C" int pb_dev_label_occupancy(uint32_t cta_threads, int *blocks_per_sm)

@@ -144,7 +144,7 @@ extern "C" int pose_b200_topo_label_noalloc(const pose_hbm_topo_t *topo, const u
         p.nbatches = (uint32_t)((p.nunits + plan.G - 1) / plan.G);
         p.queue = na.queue;
         p.one = 1;
-        if (pb_dev_label(&p, plan.grid, plan.cta, s) != 0) goto cuda_fail;
+        if (pb_dev_label(&p, plan.grid, plan.cta, 0, s) != 0) goto cuda_fail;
     }
     /* labels and seeds never outlive the call: clear the shared scratch, the
      * seed table and the session seed copy */

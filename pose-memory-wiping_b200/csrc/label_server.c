@@ -22,11 +22,18 @@
  *   - finished waves are reaped and their arena range is zeroed on the device
  *     before it is reused;
  *   - deep requests (topologies of at least PB_SERVER_DEEP_LEVELS levels,
- *     chunk_blocks 2^17 and up) do not join waves: each runs alone on the
- *     depth kernel (k_label_ws, one chunk copy per CTA, with its own producer
- *     warp) in a slot of its own, so a wave never waits for a deep request's
- *     chain and a deep request never runs on the lockstep kernel.  At most one
- *     depth CTA per SM is in flight; their scratch comes from the same arena.
+ *     chunk_blocks 2^17 and up) do not join waves: the pending deep requests
+ *     of one topology run together on the multi-unit depth kernel
+ *     (k_label_wsg: a producer warp and 15 hashing warps per CTA, 1 to 4
+ *     chunk copies per CTA) in a slot of their own, on a high-priority
+ *     stream, so a wave never waits for a deep chain and a deep chain never
+ *     runs on the lockstep kernel.  At most one depth CTA per SM is in
+ *     flight; the units per CTA grow with the load (as few as the free SMs
+ *     allow: one per CTA on an idle GPU, for the shortest chain; four under
+ *     load, for the most chains per SM).  Their scratch comes from the same
+ *     arena;
+ *   - admission never waits in line: a deep request that has to wait for
+ *     SMs or scratch does not hold back the shallow requests behind it.
  * Every request's bytes are those of labelling it alone.
  */
 #include "batch_internal.h"
@@ -43,9 +50,13 @@
 #include <time.h>
 
 #define PB_SERVER_MAX_WAVES 16
+/* Concurrent launches of the depth kernel. */
+#define PB_SERVER_MAX_DEEP 16
 /* Requests whose topology has at least this many levels (chunk_blocks 2^17
- * and up) run alone on the depth kernel instead of joining a wave. */
+ * and up) run on the depth kernel instead of joining a wave. */
 #define PB_SERVER_DEEP_LEVELS 300000u
+/* Hashing warps of a depth-kernel CTA. */
+#define PB_SERVER_DEEP_WARPS 15u
 
 typedef struct {
     const pose_hbm_topo_t *topo;
@@ -53,6 +64,7 @@ typedef struct {
     size_t len;
     uint64_t rbo;
     int session;
+    int deep;  /* runs on the depth kernel */
     int state; /* 0 pending, 1 running, 2 done, 3 failed */
     double t_submit, t_start, t_done;
 } sreq_t;
@@ -70,7 +82,7 @@ typedef struct {
     unsigned int *h_done;      /* mapped host counters, one per request */
     unsigned int *d_done;
     size_t done_cap;
-    int deep;                  /* one deep request on the depth kernel (completes with the launch) */
+    int deep;                  /* deep requests on the depth kernel (complete with the launch) */
     uint32_t ctas;             /* its CTAs, one SM each */
 } wave_t;
 
@@ -93,8 +105,11 @@ struct pose_b200_server {
     uint64_t free_off[2 * PB_SERVER_MAX_WAVES + 2], free_len[2 * PB_SERVER_MAX_WAVES + 2];
     int nfree;
     wave_t waves[PB_SERVER_MAX_WAVES];
+    wave_t deeps[PB_SERVER_MAX_DEEP]; /* depth-kernel launches, high-priority streams */
     uint32_t max_waves;        /* concurrent multi-topology waves */
     uint32_t deep_ctas;        /* depth-kernel CTAs in flight */
+    uint32_t sms;
+    uint32_t wsg_smem_max;     /* the depth kernel's shared-memory limit (0: no depth kernel) */
     int occ;
     uint64_t waves_launched;
     double busy_ms;
@@ -155,147 +170,243 @@ static void arena_give(pose_b200_server_t *s, uint64_t off, uint64_t len)
     }
 }
 
-/* A request that runs alone on the depth kernel: a deep topology that has
- * the depth kernel's records, whose scratch for one chunk copy fits the
- * arena (otherwise it joins a wave like the others). */
-static int req_is_deep(const pose_b200_server_t *s, const sreq_t *r)
+/* Whether a request runs on the depth kernel: a deep topology whose 512-slot
+ * records the multi-unit depth kernel has (built here on first use: call
+ * without the server lock held), on a GPU whose CTAs hold the kernel's
+ * shared memory, with one chunk copy's scratch fitting the arena
+ * (otherwise it joins a wave like the others). */
+static int req_is_deep(const pose_b200_server_t *s, const pose_hbm_topo_t *topo)
 {
     pb_topo_internal_t ti;
-    const uint64_t per = pb_topo_depth_unit_scratch(r->topo);
-    return pb_topo_internal(r->topo, &ti) == 0 && ti.view.L >= PB_SERVER_DEEP_LEVELS && per > 0 &&
-           per <= s->arena_bytes;
+    pb_topo_view2_t v2;
+    if (!s->wsg_smem_max || pb_topo_internal(topo, &ti) != 0 || ti.view.L < PB_SERVER_DEEP_LEVELS) return 0;
+    if (pb_topo_view2_small(topo, &v2) != 0) {
+        cudaGetLastError();
+        return 0;
+    }
+    return pb_wsg_smem_bytes(v2.csm, 4, PB_SERVER_DEEP_WARPS) <= s->wsg_smem_max &&
+           (uint64_t)v2.gpool * 32 <= s->arena_bytes;
 }
 
-/* With the lock held: launch the oldest pending request (a deep one) alone
- * on the depth kernel, one chunk copy per CTA and CTA per SM, in a free wave
- * slot.  Its CTAs count against the SMs (at most one depth CTA per SM in
- * flight) and its scratch comes from the arena.  It completes when its
- * launch does.  Returns 1 when it was launched (or failed), 0 when it has to
- * wait for a slot, SMs or scratch. */
+/* Device tables of one launch in a slot's buffer, grown on demand. */
+static int slot_tables(wave_t *wv, size_t total)
+{
+    if (wv->tables_cap >= total) return 0;
+    cudaFree(wv->d_tables);
+    wv->d_tables = NULL;
+    wv->tables_cap = 0;
+    if (pb_dev_malloc(&wv->d_tables, total * 2) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    wv->tables_cap = total * 2;
+    return 0;
+}
+
+static int slot_reqs(wave_t *wv, size_t n)
+{
+    if (wv->reqs_cap >= n) return 0;
+    uint64_t *nr = (uint64_t *)realloc(wv->reqs, n * sizeof(uint64_t));
+    if (nr) wv->reqs = nr;
+    uint32_t *nn = nr ? (uint32_t *)realloc(wv->need, n * sizeof(uint32_t)) : NULL;
+    if (nn) wv->need = nn;
+    if (!nr || !nn) return -1;
+    wv->reqs_cap = n;
+    return 0;
+}
+
+/* With the lock held: launch the pending deep requests of the oldest pending
+ * deep request's topology, oldest first, on the multi-unit depth kernel in a
+ * free deep slot.  G units per CTA, as few as the free SMs allow (a CTA per
+ * SM at most: the CTAs in flight count against the SMs), so one CTA runs one
+ * copy's chain on an idle GPU and four under load; the CTAs pull the
+ * launch's batches from a queue.  Requests are taken while they fit four
+ * units per free SM (the first always).  The requests complete with the
+ * launch.  Returns 1 when something was launched (or failed), 0 when it has
+ * to wait for a slot, SMs or scratch. */
 static int admit_deep(pose_b200_server_t *s)
 {
-    const size_t idx = s->next_pending;
-    sreq_t *r = &s->reqs[idx];
+    size_t i0 = s->next_pending;
+    while (i0 < s->nreqs && !(s->reqs[i0].state == 0 && s->reqs[i0].deep)) i0++;
+    if (i0 >= s->nreqs) return 0;
+    int w = -1;
+    for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP && w < 0; i++) if (!s->deeps[i].busy) w = (int)i;
+    if (w < 0 || s->deep_ctas >= s->sms) return 0;
+    const pose_hbm_topo_t *topo = s->reqs[i0].topo;
     pb_topo_internal_t ti;
-    if (pb_topo_internal(r->topo, &ti) != 0) return 0;
-    const uint64_t nsuper = r->len / ti.super_bytes;
-    if (nsuper == 0) { /* nothing to label */
-        r->state = 2;
-        r->t_start = r->t_done = now_ms();
-        s->next_pending++;
+    pb_topo_view2_t v2;
+    if (pb_topo_internal(topo, &ti) != 0 || pb_topo_view2_small(topo, &v2) != 0) return 0;
+    const uint32_t free_sms = s->sms - s->deep_ctas;
+    /* the group: same topology, oldest first, while four units per free SM hold them */
+    size_t n = 0;
+    uint64_t units = 0, nsuper = 0;
+    for (size_t i = i0; i < s->nreqs; i++) {
+        const sreq_t *r = &s->reqs[i];
+        if (r->state != 0 || !r->deep || r->topo != topo) continue;
+        const uint64_t ns = r->len / ti.super_bytes;
+        if (n > 0 && units + ns * ti.copies > 4ull * free_sms) break;
+        units += ns * ti.copies;
+        nsuper += ns;
+        n++;
+    }
+    wave_t *wv = &s->deeps[w];
+    if (slot_reqs(wv, n) != 0) return 0;
+    {
+        size_t k = 0;
+        for (size_t i = i0; i < s->nreqs && k < n; i++) {
+            const sreq_t *r = &s->reqs[i];
+            if (r->state == 0 && r->deep && r->topo == topo) wv->reqs[k++] = i;
+        }
+    }
+    const double t = now_ms();
+    if (units == 0) { /* nothing to label */
+        for (size_t k = 0; k < n; k++) {
+            sreq_t *r = &s->reqs[wv->reqs[k]];
+            r->state = 2;
+            r->t_start = r->t_done = t;
+        }
         pthread_cond_broadcast(&s->cv);
         return 1;
     }
-    int w = -1;
-    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES && w < 0; i++) if (!s->waves[i].busy) w = (int)i;
-    const uint32_t sms = ti.sms > 0 ? (uint32_t)ti.sms : 1;
-    if (w < 0 || s->deep_ctas >= sms) return 0;
-    const uint64_t units = nsuper * ti.copies;
-    uint32_t grid = (uint32_t)(units < sms - s->deep_ctas ? units : sms - s->deep_ctas);
-    const uint64_t per = pb_topo_depth_unit_scratch(r->topo);
+    /* an idle depth kernel runs the group at the fewest units per CTA that
+     * fit the free SMs (the shortest chains); while other depth work runs or
+     * waits, four per CTA (the most chains per SM: four units' narrow levels
+     * still take one warp pass) */
+    size_t pending_deep = 0;
+    for (size_t i = i0; i < s->nreqs; i++) pending_deep += s->reqs[i].state == 0 && s->reqs[i].deep;
+    const int more = s->deep_ctas > 0 || pending_deep > n;
+    uint32_t G = more ? 4u : (uint32_t)((units + free_sms - 1) / free_sms);
+    if (G < 1) G = 1;
+    if (G > 4) G = 4;
+    const uint64_t nbatches = (units + G - 1) / G;
+    uint32_t grid = (uint32_t)(nbatches < free_sms ? nbatches : free_sms);
+    const uint64_t per = (uint64_t)v2.gpool * 32 * G;
     const uint64_t fit = arena_largest(s) / per;
     if (fit < grid) grid = (uint32_t)fit;
     if (grid == 0) return 0; /* wait for scratch */
-    wave_t *wv = &s->waves[w];
     const uint64_t scratch = (uint64_t)grid * per;
     uint64_t off = 0;
     if (arena_take(s, scratch, &off) != 0) return 0;
-    /* tables: jobs | seeds | queue, 256-byte aligned */
-    const size_t o_jobs = 0, o_seeds = (nsuper * sizeof(pb_seedjob_t) + 255) & ~(size_t)255;
-    const size_t o_queue = (o_seeds + nsuper * 32 + 255) & ~(size_t)255, total = o_queue + 256;
-    pb_seedjob_t *jobs = (pb_seedjob_t *)malloc(nsuper * sizeof(pb_seedjob_t));
-    if (!jobs) { arena_give(s, off, scratch); return 0; }
-    if (wv->tables_cap < total) {
-        cudaFree(wv->d_tables);
-        wv->d_tables = NULL;
-        wv->tables_cap = 0;
-        if (pb_dev_malloc(&wv->d_tables, total * 2) != cudaSuccess) {
-            cudaGetLastError();
-            free(jobs);
-            arena_give(s, off, scratch);
-            return 0;
+    /* tables: units | jobs | seeds | queue, 256-byte aligned */
+#define AL(x) (((x) + 255) & ~(size_t)255)
+    const size_t o_units = 0, o_jobs = AL(units * sizeof(pb_munit_t));
+    const size_t o_seeds = AL(o_jobs + nsuper * sizeof(pb_seedjob_t)), o_queue = AL(o_seeds + nsuper * 32);
+    const size_t total = AL(o_queue + 64);
+#undef AL
+    pb_munit_t *hu = (pb_munit_t *)malloc(units * sizeof(pb_munit_t));
+    pb_seedjob_t *hj = (pb_seedjob_t *)malloc(nsuper * sizeof(pb_seedjob_t));
+    if (!hu || !hj || slot_tables(wv, total) != 0) {
+        free(hu);
+        free(hj);
+        arena_give(s, off, scratch);
+        return 0;
+    }
+    {
+        uint64_t u = 0, j = 0;
+        for (size_t k = 0; k < n; k++) {
+            const sreq_t *r = &s->reqs[wv->reqs[k]];
+            const uint64_t ns = r->len / ti.super_bytes;
+            for (uint64_t c = 0; c < ns; c++, j++) {
+                hj[j].chunk_index = (r->rbo + c * (uint64_t)ti.cb) / ti.cb;
+                hj[j].seed_off = s->sess_off[r->session];
+                hj[j].seed_len = s->sess_len[r->session];
+                for (uint32_t cp = 0; cp < ti.copies; cp++, u++) {
+                    hu[u].out = (uint64_t)(uintptr_t)r->dev_ptr + c * ti.super_bytes;
+                    hu[u].seed = (uint32_t)j;
+                    hu[u].copy = cp;
+                }
+            }
         }
-        wv->tables_cap = total * 2;
-    }
-    if (wv->reqs_cap < 1) {
-        uint64_t *nr = (uint64_t *)realloc(wv->reqs, sizeof(uint64_t));
-        if (!nr) { free(jobs); arena_give(s, off, scratch); return 0; }
-        wv->reqs = nr;
-        wv->reqs_cap = 1;
-    }
-    for (uint64_t j = 0; j < nsuper; j++) {
-        jobs[j].chunk_index = (r->rbo + j * (uint64_t)ti.cb) / ti.cb;
-        jobs[j].seed_off = s->sess_off[r->session];
-        jobs[j].seed_len = s->sess_len[r->session];
     }
     uint8_t *T = (uint8_t *)wv->d_tables;
-    uint32_t *d_seeds = (uint32_t *)(T + o_seeds);
-    int ok = cudaMemcpyAsync(T + o_jobs, jobs, nsuper * sizeof(pb_seedjob_t), cudaMemcpyHostToDevice, wv->stream) ==
+    int ok = cudaMemcpyAsync(T + o_units, hu, units * sizeof(pb_munit_t), cudaMemcpyHostToDevice, wv->stream) ==
              cudaSuccess;
-    /* the upload reads `jobs`: wait for it before freeing them */
+    ok = ok && cudaMemcpyAsync(T + o_jobs, hj, nsuper * sizeof(pb_seedjob_t), cudaMemcpyHostToDevice, wv->stream) ==
+                   cudaSuccess;
+    /* the uploads read the host tables: wait for them before freeing them */
     ok = ok && cudaStreamSynchronize(wv->stream) == cudaSuccess;
-    free(jobs);
-    ok = ok && pb_dev_seed_jobs(T + o_jobs, (uint32_t)nsuper, s->d_sessions, d_seeds, wv->stream) == 0;
+    free(hu);
+    free(hj);
+    ok = ok && pb_dev_seed_jobs(T + o_jobs, (uint32_t)nsuper, s->d_sessions, (uint32_t *)(T + o_seeds), wv->stream) == 0;
     ok = ok && cudaMemsetAsync(T + o_queue, 0, 64, wv->stream) == cudaSuccess;
-    ok = ok && pb_topo_launch_depth(r->topo, d_seeds, r->dev_ptr, nsuper, s->d_arena + off, grid,
-                                    (unsigned int *)(T + o_queue), wv->stream) == 0;
-    /* scratch and chunk seeds are zeroed before the request counts as done */
+    if (ok) {
+        pb_wsg_params_t p;
+        memset(&p, 0, sizeof(p));
+        p.topo = v2;
+        p.units = (const pb_munit_t *)(T + o_units);
+        p.seeds = (const uint32_t *)(T + o_seeds);
+        p.scratch = s->d_arena + off;
+        p.unit_scratch_bytes = (uint64_t)v2.gpool * 32;
+        p.nunits = (uint32_t)units;
+        p.units_per_cta = G;
+        p.team_warps = PB_SERVER_DEEP_WARPS;
+        p.nbatches = (uint32_t)nbatches;
+        p.queue = (unsigned int *)(T + o_queue);
+        ok = pb_dev_label_wsg(&p, grid, 32 * (PB_SERVER_DEEP_WARPS + 1),
+                              pb_wsg_smem_bytes(v2.csm, G, PB_SERVER_DEEP_WARPS), wv->stream) == 0;
+    }
+    /* scratch and chunk seeds are zeroed before the requests count as done */
     ok = ok && cudaMemsetAsync(s->d_arena + off, 0, scratch, wv->stream) == cudaSuccess;
-    ok = ok && cudaMemsetAsync(d_seeds, 0, nsuper * 32, wv->stream) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(T + o_seeds, 0, nsuper * 32, wv->stream) == cudaSuccess;
     ok = ok && cudaEventRecord(wv->done, wv->stream) == cudaSuccess;
-    const double t = now_ms();
     if (!ok) {
         fprintf(stderr, "pose_b200_server: deep launch failed: %s\n", cudaGetErrorString(cudaGetLastError()));
         cudaStreamSynchronize(wv->stream);
         cudaMemsetAsync(s->d_arena + off, 0, scratch, wv->stream);
-        cudaMemsetAsync(d_seeds, 0, nsuper * 32, wv->stream);
+        cudaMemsetAsync(T + o_seeds, 0, nsuper * 32, wv->stream);
         cudaStreamSynchronize(wv->stream);
         cudaGetLastError();
         arena_give(s, off, scratch);
-        r->state = 3;
-        r->t_done = t;
+        for (size_t k = 0; k < n; k++) {
+            s->reqs[wv->reqs[k]].state = 3;
+            s->reqs[wv->reqs[k]].t_done = t;
+        }
     } else {
         wv->busy = 1;
         wv->deep = 1;
         wv->ctas = grid;
         wv->arena_off = off;
         wv->arena_len = scratch;
-        wv->nreqs = 1;
-        wv->reqs[0] = idx;
+        wv->nreqs = n;
         s->deep_ctas += grid;
-        r->state = 1;
-        r->t_start = t;
+        for (size_t k = 0; k < n; k++) {
+            s->reqs[wv->reqs[k]].state = 1;
+            s->reqs[wv->reqs[k]].t_start = t;
+        }
         s->waves_launched++;
     }
-    s->next_pending++;
     pthread_cond_broadcast(&s->cv);
     return 1;
 }
 
-/* With the lock held: launch one wave from the oldest pending requests.
- * Returns 1 when a wave was launched, 0 when nothing could be admitted. */
-static int admit(pose_b200_server_t *s)
+/* With the lock held: launch one wave from every pending request that does
+ * not run on the depth kernel.  Returns 1 when a wave was launched (or its
+ * requests failed), 0 when nothing could be admitted. */
+static int admit_wave(pose_b200_server_t *s)
 {
-    if (s->next_pending >= s->nreqs) return 0;
-    if (req_is_deep(s, &s->reqs[s->next_pending])) return admit_deep(s);
     int w = -1;
     uint32_t multi = 0;
     for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
-        if (s->waves[i].busy) multi += !s->waves[i].deep;
+        if (s->waves[i].busy) multi++;
         else if (w < 0) w = (int)i;
     }
     if (w < 0 || multi >= s->max_waves) return 0;
     wave_t *wv = &s->waves[w];
     wv->deep = 0;
     wv->ctas = 0;
-    /* take everything pending up to the next deep request */
-    size_t first = s->next_pending, last = first;
-    while (last < s->nreqs && !req_is_deep(s, &s->reqs[last])) last++;
-    size_t n = last - first;
+    size_t n = 0;
+    for (size_t i = s->next_pending; i < s->nreqs; i++) n += s->reqs[i].state == 0 && !s->reqs[i].deep;
+    if (n == 0) return 0;
+    if (slot_reqs(wv, n) != 0) return 0;
+    {
+        size_t k = 0;
+        for (size_t i = s->next_pending; i < s->nreqs && k < n; i++)
+            if (s->reqs[i].state == 0 && !s->reqs[i].deep) wv->reqs[k++] = i;
+    }
     pb_req_t *pr = (pb_req_t *)calloc(n, sizeof(*pr));
     if (!pr) return 0;
     for (size_t i = 0; i < n; i++) {
-        const sreq_t *r = &s->reqs[first + i];
+        const sreq_t *r = &s->reqs[wv->reqs[i]];
         pr[i].topo = r->topo;
         pr[i].dev_ptr = r->dev_ptr;
         pr[i].len = r->len;
@@ -308,16 +419,18 @@ static int admit(pose_b200_server_t *s)
     double eff = 0.0;
     if (pb_plan_choose(pr, n, NULL, &Tw, &eff) != 0 || pb_plan_requests(pr, n, Tw, 32, eff, &pl) != 0) {
         free(pr);
-        for (size_t i = first; i < last; i++) { s->reqs[i].state = 3; s->reqs[i].t_done = now_ms(); }
-        s->next_pending = last;
+        for (size_t i = 0; i < n; i++) { s->reqs[wv->reqs[i]].state = 3; s->reqs[wv->reqs[i]].t_done = now_ms(); }
         pthread_cond_broadcast(&s->cv);
         return 1;
     }
     free(pr);
     int launched = 0;
     if (pl.nunits == 0) { /* nothing to label: done at once */
-        for (size_t i = first; i < last; i++) { s->reqs[i].state = 2; s->reqs[i].t_start = s->reqs[i].t_done = now_ms(); }
-        s->next_pending = last;
+        for (size_t i = 0; i < n; i++) {
+            sreq_t *r = &s->reqs[wv->reqs[i]];
+            r->state = 2;
+            r->t_start = r->t_done = now_ms();
+        }
         pthread_cond_broadcast(&s->cv);
         pb_plan_free(&pl);
         return 1;
@@ -354,14 +467,6 @@ static int admit(pose_b200_server_t *s)
         }
         wv->done_cap = cap;
     }
-    if (wv->reqs_cap < n) {
-        uint64_t *nr = (uint64_t *)realloc(wv->reqs, n * sizeof(uint64_t));
-        if (nr) wv->reqs = nr;
-        uint32_t *nn = nr ? (uint32_t *)realloc(wv->need, n * sizeof(uint32_t)) : NULL;
-        if (nn) wv->need = nn;
-        if (!nr || !nn) { arena_give(s, off, scratch); pb_plan_free(&pl); return 0; }
-        wv->reqs_cap = n;
-    }
     memset((void *)wv->h_done, 0, n * sizeof(unsigned int));
     memset(wv->need, 0, n * sizeof(uint32_t));
     for (uint64_t u = 0; u < pl.nunits; u++) wv->need[pl.unit_req[u]]++;
@@ -376,13 +481,7 @@ static int admit(pose_b200_server_t *s)
     o_queue = AL(o_seeds + pl.njobs * 32);
     total = AL(o_queue + 64);
 #undef AL
-    if (wv->tables_cap < total) {
-        cudaFree(wv->d_tables);
-        wv->d_tables = NULL;
-        wv->tables_cap = 0;
-        if (pb_dev_malloc(&wv->d_tables, total * 2) != cudaSuccess) { arena_give(s, off, scratch); pb_plan_free(&pl); return 0; }
-        wv->tables_cap = total * 2;
-    }
+    if (slot_tables(wv, total) != 0) { arena_give(s, off, scratch); pb_plan_free(&pl); return 0; }
     uint8_t *T = (uint8_t *)wv->d_tables;
     int ok = 1;
     ok &= cudaMemcpyAsync(T + o_views, pl.views, pl.ntopo * sizeof(pb_topo_view_t), cudaMemcpyHostToDevice, wv->stream) == cudaSuccess;
@@ -423,24 +522,34 @@ static int admit(pose_b200_server_t *s)
         cudaStreamSynchronize(wv->stream);
         cudaGetLastError();
         arena_give(s, off, scratch);
-        for (size_t i = first; i < last; i++) { s->reqs[i].state = 3; s->reqs[i].t_done = t; }
+        for (size_t i = 0; i < n; i++) { s->reqs[wv->reqs[i]].state = 3; s->reqs[wv->reqs[i]].t_done = t; }
     } else {
         wv->busy = 1;
         wv->arena_off = off;
         wv->arena_len = scratch;
         wv->nreqs = n;
         for (size_t i = 0; i < n; i++) {
-            wv->reqs[i] = first + i;
-            s->reqs[first + i].state = 1;
-            s->reqs[first + i].t_start = t;
+            s->reqs[wv->reqs[i]].state = 1;
+            s->reqs[wv->reqs[i]].t_start = t;
         }
         s->waves_launched++;
         launched = 1;
     }
-    s->next_pending = last;
     pb_plan_free(&pl);
     pthread_cond_broadcast(&s->cv);
     return launched || !ok;
+}
+
+/* With the lock held: one round of admission — deep requests first (their
+ * chains are the long poles), then a wave of the rest.  Returns 1 when
+ * anything changed. */
+static int admit(pose_b200_server_t *s)
+{
+    while (s->next_pending < s->nreqs && s->reqs[s->next_pending].state != 0) s->next_pending++;
+    if (s->next_pending >= s->nreqs) return 0;
+    const int d = admit_deep(s);
+    const int w = admit_wave(s);
+    return d || w;
 }
 
 /* With the lock held: complete the requests whose chunk copies are all in,
@@ -448,8 +557,8 @@ static int admit(pose_b200_server_t *s)
 static int reap(pose_b200_server_t *s)
 {
     int k = 0;
-    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
-        wave_t *wv = &s->waves[i];
+    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES + PB_SERVER_MAX_DEEP; i++) {
+        wave_t *wv = i < PB_SERVER_MAX_WAVES ? &s->waves[i] : &s->deeps[i - PB_SERVER_MAX_WAVES];
         if (!wv->busy) continue;
         double t = now_ms();
         for (size_t r = 0; r < wv->nreqs && !wv->deep; r++) {
@@ -483,20 +592,26 @@ static int reap(pose_b200_server_t *s)
     return k;
 }
 
+static int any_busy(const pose_b200_server_t *s)
+{
+    int busy = 0;
+    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) busy |= s->waves[i].busy;
+    for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP; i++) busy |= s->deeps[i].busy;
+    return busy;
+}
+
 static void *dispatcher(void *arg)
 {
     pose_b200_server_t *s = (pose_b200_server_t *)arg;
     cudaSetDevice(s->device);
     pthread_mutex_lock(&s->mu);
     for (;;) {
-        int busy = 0;
-        for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) busy |= s->waves[i].busy;
-        if (!s->running && !busy && s->next_pending >= s->nreqs) break;
+        while (s->next_pending < s->nreqs && s->reqs[s->next_pending].state != 0) s->next_pending++;
+        if (!s->running && !any_busy(s) && s->next_pending >= s->nreqs) break;
         int progress = reap(s);
         while (admit(s)) progress = 1;
         if (!progress) {
-            busy = 0;
-            for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) busy |= s->waves[i].busy;
+            const int busy = any_busy(s);
             struct timespec ts;
             clock_gettime(CLOCK_REALTIME, &ts);
             long ns = busy ? 50000 : 2000000; /* poll running waves every 50 us */
@@ -540,6 +655,27 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
             cudaEventCreateWithFlags(&s->waves[i].done, cudaEventDisableTiming) != cudaSuccess)
             goto fail;
     }
+    {
+        /* depth-kernel launches get the highest stream priority: when a
+         * wave's CTA leaves an SM, a waiting depth CTA takes it first */
+        int lo = 0, hi = 0;
+        if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) lo = hi = 0;
+        for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP; i++) {
+            if (cudaStreamCreateWithPriority(&s->deeps[i].stream, cudaStreamNonBlocking, hi) != cudaSuccess ||
+                cudaEventCreateWithFlags(&s->deeps[i].done, cudaEventDisableTiming) != cudaSuccess)
+                goto fail;
+        }
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess || sms <= 0) sms = 1;
+        /* POSE_B200_SERVER_DEEP_SMS caps the SMs the depth kernel may hold (tests, tuning) */
+        const char *e = getenv("POSE_B200_SERVER_DEEP_SMS");
+        if (e && atoi(e) > 0 && atoi(e) < sms) sms = atoi(e);
+        s->sms = (uint32_t)sms;
+        uint32_t mx = 0;
+        if (pb_dev_label_wsg_prepare(&mx) != 0) mx = 0; /* no depth kernel: deep requests join waves */
+        cudaGetLastError();
+        s->wsg_smem_max = mx;
+    }
     if (pb_dev_label_multi_occupancy(256, &s->occ) != 0) s->occ = 1;
     s->running = 1;
     if (pthread_create(&s->thread, NULL, dispatcher, s) != 0) { s->running = 0; goto fail; }
@@ -549,6 +685,10 @@ fail:
     for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
         if (s->waves[i].stream) cudaStreamDestroy(s->waves[i].stream);
         if (s->waves[i].done) cudaEventDestroy(s->waves[i].done);
+    }
+    for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP; i++) {
+        if (s->deeps[i].stream) cudaStreamDestroy(s->deeps[i].stream);
+        if (s->deeps[i].done) cudaEventDestroy(s->deeps[i].done);
     }
     cudaFree(s->d_arena);
     pthread_mutex_destroy(&s->mu);
@@ -569,9 +709,8 @@ int pose_b200_server_session(pose_b200_server_t *s, const uint8_t *seed, size_t 
      * reading their own copy until they finish, so growth waits for idle) */
     if (s->sess_bytes + seed_len > s->sess_cap) {
         for (;;) {
-            int busy = 0;
-            for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) busy |= s->waves[i].busy;
-            if (!busy && s->next_pending >= s->nreqs) break;
+            while (s->next_pending < s->nreqs && s->reqs[s->next_pending].state != 0) s->next_pending++;
+            if (!any_busy(s) && s->next_pending >= s->nreqs) break;
             pthread_cond_wait(&s->cv, &s->mu);
         }
         size_t ncap = (s->sess_cap ? s->sess_cap * 2 : 4096);
@@ -608,10 +747,19 @@ out:
     return id;
 }
 
+int pose_b200_server_prepare(pose_b200_server_t *s, const pose_hbm_topo_t *topo)
+{
+    if (!s || !topo) return -1;
+    (void)req_is_deep(s, topo); /* builds the depth kernel's records of a deep topology */
+    return 0;
+}
+
 int64_t pose_b200_server_submit(pose_b200_server_t *s, const pose_hbm_topo_t *topo, int session, void *dev_ptr,
                                 size_t len, uint64_t region_block_offset)
 {
     if (!s || !topo) return -1;
+    /* before the lock: a deep topology's first request builds its records */
+    const int deep = req_is_deep(s, topo);
     pthread_mutex_lock(&s->mu);
     int64_t id = -1;
     if (session < 0 || (size_t)session >= s->nsess) {
@@ -648,6 +796,7 @@ int64_t pose_b200_server_submit(pose_b200_server_t *s, const pose_hbm_topo_t *to
     r->len = len;
     r->rbo = region_block_offset;
     r->session = session;
+    r->deep = deep;
     r->t_submit = now_ms();
     id = (int64_t)s->nreqs++;
     pthread_cond_broadcast(&s->cv);
@@ -696,14 +845,15 @@ void pose_b200_server_destroy(pose_b200_server_t *s)
     pthread_cond_broadcast(&s->cv);
     pthread_mutex_unlock(&s->mu);
     pthread_join(s->thread, NULL);
-    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
-        cudaStreamSynchronize(s->waves[i].stream);
-        cudaStreamDestroy(s->waves[i].stream);
-        cudaEventDestroy(s->waves[i].done);
-        cudaFree(s->waves[i].d_tables);
-        if (s->waves[i].h_done) cudaFreeHost(s->waves[i].h_done);
-        free(s->waves[i].reqs);
-        free(s->waves[i].need);
+    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES + PB_SERVER_MAX_DEEP; i++) {
+        wave_t *wv = i < PB_SERVER_MAX_WAVES ? &s->waves[i] : &s->deeps[i - PB_SERVER_MAX_WAVES];
+        cudaStreamSynchronize(wv->stream);
+        cudaStreamDestroy(wv->stream);
+        cudaEventDestroy(wv->done);
+        cudaFree(wv->d_tables);
+        if (wv->h_done) cudaFreeHost(wv->h_done);
+        free(wv->reqs);
+        free(wv->need);
     }
     if (s->d_arena) {
         cudaMemset(s->d_arena, 0, s->arena_bytes);

@@ -34,8 +34,11 @@
 #include "b3_device.cuh"
 #include "kernels.h"
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+namespace cg = cooperative_groups;
 
 namespace pb {
 namespace {
@@ -273,6 +276,127 @@ __global__ void __launch_bounds__(PB_CTA_THREADS, 1) k_label_ws(const __grid_con
     }
 }
 
+/* k_label_ws with a thread-block cluster of C CTAs per chunk copy, for
+ * launches with fewer copies than SMs.  CTA rank 0 runs the copy exactly as
+ * k_label_ws does (producer warp, shared-memory pool, a CTA barrier per
+ * level).  A level wider than split_width is shared: rank 0 hashes its
+ * staged nodes and as many of the rest as bring it to ceil(w / C) nodes; the
+ * other ranks hash the remainder, striding over it, with direct loads, and
+ * read and write rank 0's shared-memory pool through distributed shared
+ * memory.  Every boundary between levels l - 1 and l where l - 1 or l is
+ * split is a cluster barrier instead of rank 0's CTA barrier; the other
+ * ranks walk only the split levels (split_levels, nsplit of them, ascending)
+ * and meet rank 0 at exactly those barriers, so every CTA of the cluster
+ * passes the same barrier sequence.  One copy per cluster: the grid is
+ * nunits * C CTAs, and copy k's global pool is at scratch + k *
+ * team_scratch_bytes.  No spin-waits: only CTA and cluster barriers. */
+__global__ void __launch_bounds__(PB_CTA_THREADS, 1) k_label_wsc(const __grid_constant__ pb_pipe_params_t p)
+{
+    extern __shared__ uint4 smem[];
+    cg::cluster_group cl = cg::this_cluster();
+    const pb_topo_view2_t &tp = p.topo;
+    const uint32_t C = p.cluster;
+    const uint32_t rank = cl.block_rank();
+    const uint32_t unit = blockIdx.x / C;
+    const uint32_t NC = p.team_warps;
+    const uint32_t nthr = NC * 32;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool producer = warp == NC;
+    const uint32_t c = threadIdx.x;
+    const uint32_t sw = p.split_width;
+    Smem sm;
+    sm.slots = nthr;
+    sm.pool = smem;
+    sm.rec = sm.pool + (size_t)tp.csm * 2;
+    sm.dat = sm.rec + (size_t)3 * nthr * 2;
+    sm.hdr = sm.dat + (size_t)2 * nthr * 6;
+    Unit un;
+    un.gscr = reinterpret_cast<uint4 *>(p.scratch + (uint64_t)unit * p.team_scratch_bytes);
+    const uint32_t chunk = unit >> p.copies_log2;
+    un.copy = unit & ((1u << p.copies_log2) - 1u);
+    un.rank_base = un.copy ? tp.half_w : 0u;
+    un.rank_lim = un.copy ? tp.retained : tp.half_w;
+    un.out = p.persist + (uint64_t)(p.first_super + chunk) * p.super_bytes;
+    un.cv0 = tp.cv0 + (uint64_t)un.copy * tp.S * 2;
+#pragma unroll
+    for (int i = 0; i < 8; i++) un.seed[i] = p.seeds[8 * (size_t)chunk + i];
+
+    if (rank != 0) {
+        /* rank 0's pool, through distributed shared memory */
+        Smem rs;
+        rs.slots = 0;
+        rs.pool = cl.map_shared_rank(smem, 0);
+        rs.rec = rs.dat = rs.hdr = nullptr;
+        for (uint32_t k = 0; k < p.nsplit; k++) {
+            const uint32_t l = __ldg(p.split_levels + k);
+            if (k == 0 || __ldg(p.split_levels + k - 1) + 1 != l) cl.sync(); /* boundary l */
+            const uint32_t ls = __ldg(tp.lstart + l), w = __ldg(tp.lstart + l + 1) - ls;
+            const uint32_t per = (w + C - 1) / C, a = per > nthr ? per - nthr : 0;
+            if (!producer)
+                for (uint32_t j = nthr + a + (rank - 1) * nthr + c; j < w; j += (C - 1) * nthr)
+                    direct_item(p, un, rs, ls + j);
+            cl.sync(); /* boundary l + 1 */
+        }
+        return;
+    }
+
+    /* rank 0: prologue as k_label_ws */
+    if (producer) {
+        stage_records(p, sm, 0, lane);
+        stage_records(p, sm, 1, lane);
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncwarp();
+        const uint32_t ls0 = __ldg(tp.lstart), w0 = __ldg(tp.lstart + 1) - ls0;
+        stage_data(p, sm, un, 0, ls0, w0, lane);
+        cp_async_commit();
+        cp_async_wait_all();
+    }
+    __syncthreads();
+    if (tp.L > 0 && __ldg(tp.lstart + 1) - __ldg(tp.lstart) > sw) cl.sync(); /* boundary 0 */
+
+    for (uint32_t l = 0; l < tp.L; l++) {
+        const uint4 h = sm.hdr[l % 3];
+        const uint32_t ls = h.x, w = h.y;
+        /* the next level's width (its header arrived during level l - 1) */
+        const uint32_t wn = l + 1 < tp.L ? sm.hdr[(l + 1) % 3].y : 0u;
+        if (producer) {
+            stage_records(p, sm, l + 2, lane);
+            if (l + 1 < tp.L) stage_data(p, sm, un, l + 1, sm.hdr[(l + 1) % 3].x, wn, lane);
+            cp_async_commit();
+            cp_async_wait_all();
+        } else {
+            if (c < w && c < nthr) {
+                const uint4 r0 = *sm.r(l % 3, c), r1 = *(sm.r(l % 3, c) + 1);
+                const uint4 *d = sm.d(l & 1, c);
+                const uint32_t np = (r0.x >> PB_REC_NP_SHIFT) & 3u;
+                uint32_t m[16], cv[8];
+#pragma unroll
+                for (int i = 0; i < 16; i++) m[i] = 0;
+                if (np >= 1) {
+                    if (r0.y & PB_REF_PREV) load_prev(un, sm, r0.y, m);
+                    else put8(m, d[2], d[3]);
+                }
+                if (np >= 2) {
+                    if (r0.z & PB_REF_PREV) load_prev(un, sm, r0.z, m + 8);
+                    else put8(m + 8, d[4], d[5]);
+                }
+                put8(cv, d[0], d[1]);
+                hash_node(p, un, cv, m);
+                store_label(un, sm, r0, r1, cv);
+            }
+            uint32_t lim = w;
+            if (w > sw) { /* split: rank 0 stops at ceil(w / C) nodes */
+                const uint32_t per = (w + C - 1) / C, a = per > nthr ? per - nthr : 0;
+                lim = nthr + a < w ? nthr + a : w;
+            }
+            for (uint32_t j = c + nthr; j < lim; j += nthr) direct_item(p, un, sm, ls + j);
+        }
+        if (w > sw || wn > sw) cl.sync(); /* boundary l + 1 */
+        else __syncthreads();
+    }
+}
+
 namespace {
 
 /* Shared-memory layout of the multi-unit kernel (uint4 units):
@@ -280,8 +404,8 @@ namespace {
  *   rec   [3][slots][2] records of up to `slots` nodes per level (shared by the units)
  *   dat   [2][items][6] cv0 (2), predecessor 0 (2), predecessor 1 (2) per item
  *   hdr   [3]           (level start, width) of each ring stage
- * items = hashing threads, slots = items / G; item i is node i >> g_log2 of
- * the batch's unit i & (G - 1). */
+ * slots = hashing threads / G, items = slots * G; item i is node i / G of
+ * the batch's unit i % G. */
 struct SmemG {
     uint4 *pool, *rec, *dat, *hdr;
     uint32_t slots, items;
@@ -291,16 +415,20 @@ struct SmemG {
 
 /* Producer: block-0 values and older predecessors of level `lv` into data
  * stage lv & 1, for every item of the level's staged nodes whose unit is in
- * the batch (cnt units; s_copy = their copies). */
+ * the batch (cnt units; s_copy = their copies).  The lanes stride over the
+ * level's items, so a narrow level of G units is one pass; item i is node
+ * i / G (a multiply-high by ginv = ceil(2^32 / G), exact for these counts)
+ * of unit i % G. */
 __device__ __forceinline__ void stage_data_g(const pb_wsg_params_t &p, const SmemG &sm, const uint32_t *s_copy,
-                                             uint32_t cnt, uint32_t lv, uint32_t ls, uint32_t w, uint32_t lane)
+                                             uint32_t cnt, uint32_t lv, uint32_t ls, uint32_t w, uint32_t lane,
+                                             uint32_t ginv)
 {
     if (lv >= p.topo.L) return;
-    const uint32_t G = 1u << p.g_log2;
+    const uint32_t G = p.units_per_cta;
     const uint32_t ns = w < sm.slots ? w : sm.slots;
     const uint32_t rs = lv % 3, ds = lv & 1;
-    for (uint32_t i = lane; i < (ns << p.g_log2); i += 32) {
-        const uint32_t j = i >> p.g_log2, u = i & (G - 1);
+    for (uint32_t i = lane; i < ns * G; i += 32) {
+        const uint32_t j = G == 1 ? i : __umulhi(i, ginv), u = i - j * G;
         if (u >= cnt) continue;
         const uint4 r0 = *sm.r(rs, j);
         uint4 *d = sm.d(ds, i);
@@ -325,12 +453,12 @@ __device__ __forceinline__ void stage_data_g(const pb_wsg_params_t &p, const Sme
 
 } /* namespace */
 
-/* k_label_ws with G units of one topology per CTA.  The producer warp stages
- * each level's records once for all units and the block-0 values and older
- * predecessors of every (node, unit) item; hashing thread c works item c
- * (node c >> g_log2 of unit c & (G - 1)) and, on levels wider than the
- * staged slots, that unit's further nodes with direct loads.  One CTA
- * barrier ends a level, as in k_label_ws; there are no spin-waits. */
+/* k_label_ws with G (1 to 4) units of one topology per CTA.  The producer
+ * warp stages each level's records once for all units and the block-0
+ * values and older predecessors of every (node, unit) item; hashing thread
+ * c < slots * G works item c (node c / G of unit c % G) and, on levels wider
+ * than the staged slots, that unit's further nodes with direct loads.  One
+ * CTA barrier ends a level, as in k_label_ws; there are no spin-waits. */
 __global__ void __launch_bounds__(PB_CTA_THREADS, 1) k_label_wsg(const __grid_constant__ pb_wsg_params_t p)
 {
     extern __shared__ uint4 smem[];
@@ -339,14 +467,15 @@ __global__ void __launch_bounds__(PB_CTA_THREADS, 1) k_label_wsg(const __grid_co
     const pb_topo_view2_t &tp = p.topo;
     const uint32_t NC = p.team_warps;
     const uint32_t nthr = NC * 32;
-    const uint32_t G = 1u << p.g_log2;
+    const uint32_t G = p.units_per_cta;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool producer = warp == NC;
     const uint32_t c = threadIdx.x;
-    const uint32_t u = c & (G - 1), j0 = c >> p.g_log2;
+    const uint32_t u = c % G, j0 = c / G;
+    const uint32_t ginv = G > 1 ? (uint32_t)((0x100000000ull + G - 1) / G) : 0u;
     SmemG sg;
-    sg.items = nthr;
-    sg.slots = nthr >> p.g_log2;
+    sg.slots = nthr / G;
+    sg.items = sg.slots * G;
     sg.pool = smem;
     sg.rec = sg.pool + (size_t)G * tp.csm * 2;
     sg.dat = sg.rec + (size_t)3 * sg.slots * 2;
@@ -364,18 +493,18 @@ __global__ void __launch_bounds__(PB_CTA_THREADS, 1) k_label_wsg(const __grid_co
             s_batch = b;
             s_cnt = 0;
             if (b < p.nbatches) {
-                const uint32_t left = p.nunits - (b << p.g_log2);
+                const uint32_t left = p.nunits - b * G;
                 s_cnt = left < G ? left : G;
-                for (uint32_t k = 0; k < s_cnt; k++) s_copy[k] = p.units[(b << p.g_log2) + k].copy;
+                for (uint32_t k = 0; k < s_cnt; k++) s_copy[k] = p.units[b * G + k].copy;
             }
         }
         __syncthreads();
         const uint32_t batch = s_batch, cnt = s_cnt;
         __syncthreads();
         if (batch >= p.nbatches) break;
-        const bool act = !producer && u < cnt;
+        const bool act = !producer && u < cnt && c < sg.items;
         if (act) {
-            const pb_munit_t mu = p.units[(batch << p.g_log2) + u];
+            const pb_munit_t mu = p.units[batch * G + u];
             un.copy = mu.copy;
             un.rank_base = mu.copy ? tp.half_w : 0u;
             un.rank_lim = mu.copy ? tp.retained : tp.half_w;
@@ -393,7 +522,7 @@ __global__ void __launch_bounds__(PB_CTA_THREADS, 1) k_label_wsg(const __grid_co
             cp_async_wait_all();
             __syncwarp();
             const uint32_t ls0 = __ldg(tp.lstart), w0 = __ldg(tp.lstart + 1) - ls0;
-            stage_data_g(p, sg, s_copy, cnt, 0, ls0, w0, lane);
+            stage_data_g(p, sg, s_copy, cnt, 0, ls0, w0, lane, ginv);
             cp_async_commit();
             cp_async_wait_all();
         }
@@ -404,7 +533,7 @@ __global__ void __launch_bounds__(PB_CTA_THREADS, 1) k_label_wsg(const __grid_co
                 stage_records(p, sg, l + 2, lane);
                 if (l + 1 < tp.L) {
                     const uint4 h = sg.hdr[(l + 1) % 3];
-                    stage_data_g(p, sg, s_copy, cnt, l + 1, h.x, h.y, lane);
+                    stage_data_g(p, sg, s_copy, cnt, l + 1, h.x, h.y, lane, ginv);
                 }
                 cp_async_commit();
                 cp_async_wait_all();
@@ -451,6 +580,58 @@ extern "C" int pb_dev_label_ws(const pb_pipe_params_t *params, uint32_t grid, ui
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
+extern "C" int pb_dev_label_wsc(const pb_pipe_params_t *params, uint32_t smem_bytes, cudaStream_t stream)
+{
+    const uint32_t C = params->cluster;
+    if (C < 2 || C > 16 || (params->team_warps != 7 && params->team_warps != 15) || params->nunits == 0)
+        return -1;
+    if (cudaFuncSetAttribute(pb::k_label_wsc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes) !=
+            cudaSuccess ||
+        (C > 8 && cudaFuncSetAttribute(pb::k_label_wsc, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                      cudaSuccess))
+        return -1;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(params->nunits * C);
+    cfg.blockDim = dim3(32 * (params->team_warps + 1));
+    cfg.dynamicSmemBytes = smem_bytes;
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaGetLastError(); /* report only this launch */
+    if (cudaLaunchKernelEx(&cfg, pb::k_label_wsc, *params) != cudaSuccess) return -1;
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+/* How many clusters of C CTAs (team_warps hashing warps + 1, smem_bytes of
+ * dynamic shared memory each) the device holds at once. */
+extern "C" int pb_dev_label_wsc_max_clusters(uint32_t C, uint32_t team_warps, uint32_t smem_bytes, int *clusters)
+{
+    *clusters = 0;
+    if (C < 2 || C > 16) return -1;
+    if (cudaFuncSetAttribute(pb::k_label_wsc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes) !=
+            cudaSuccess ||
+        (C > 8 && cudaFuncSetAttribute(pb::k_label_wsc, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                      cudaSuccess))
+        return -1;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(C * 148);
+    cfg.blockDim = dim3(32 * (team_warps + 1));
+    cfg.dynamicSmemBytes = smem_bytes;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaOccupancyMaxActiveClusters(clusters, pb::k_label_wsc, &cfg) == cudaSuccess ? 0 : -1;
+}
+
 extern "C" int pb_dev_label_ws_occupancy(uint32_t cta_threads, uint32_t smem_bytes, int *blocks_per_sm)
 {
     if (cudaFuncSetAttribute(pb::k_label_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes) !=
@@ -462,18 +643,18 @@ extern "C" int pb_dev_label_ws_occupancy(uint32_t cta_threads, uint32_t smem_byt
                : -1;
 }
 
-extern "C" uint32_t pb_wsg_smem_bytes(uint32_t csm, uint32_t g_log2, uint32_t team_warps)
+extern "C" uint32_t pb_wsg_smem_bytes(uint32_t csm, uint32_t units_per_cta, uint32_t team_warps)
 {
-    const uint32_t nthr = 32u * team_warps, slots = nthr >> g_log2;
-    return (2u * (1u << g_log2) * csm + 3u * 2u * slots + 2u * 6u * nthr + 3u) * 16u;
+    const uint32_t nthr = 32u * team_warps, slots = nthr / units_per_cta;
+    return (2u * units_per_cta * csm + 3u * 2u * slots + 2u * 6u * nthr + 3u) * 16u;
 }
 
 extern "C" int pb_dev_label_wsg(const pb_wsg_params_t *params, uint32_t grid, uint32_t cta_threads,
                                 uint32_t smem_bytes, cudaStream_t stream)
 {
-    if (params->g_log2 > 2 || (params->team_warps != 7 && params->team_warps != 15) ||
-        cta_threads != 32u * (params->team_warps + 1) ||
-        smem_bytes < pb_wsg_smem_bytes(params->topo.csm, params->g_log2, params->team_warps))
+    if (params->units_per_cta < 1 || params->units_per_cta > 4 ||
+        (params->team_warps != 7 && params->team_warps != 15) || cta_threads != 32u * (params->team_warps + 1) ||
+        smem_bytes < pb_wsg_smem_bytes(params->topo.csm, params->units_per_cta, params->team_warps))
         return -1;
     cudaGetLastError(); /* report only this launch */
     pb::k_label_wsg<<<grid, cta_threads, smem_bytes, stream>>>(*params);

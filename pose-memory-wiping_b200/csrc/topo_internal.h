@@ -42,17 +42,6 @@ int pb_topo_label_raw(const pose_hbm_topo_t *t, const uint8_t *chunk_seeds, void
  * Needs a topology built with its block-0 table.  Returns 0 or -1. */
 int pb_topo_view2_small(const pose_hbm_topo_t *t, pb_topo_view2_t *out);
 
-/* The depth kernel (k_label_ws, one chunk copy per CTA) for a caller that
- * manages its own stream, scratch and chunk seeds: global scratch per chunk
- * copy (0 when the topology has no pipelined records or block-0 table), and
- * an asynchronous launch over the nsuper whole super-chunks at dev_ptr with
- * chunk seeds d_seeds (8 words per super-chunk), `grid` CTAs whose scratch is
- * grid x the per-copy size at `scratch`, and a zeroed work counter d_queue.
- * Returns 0, or -1 when the launch is refused. */
-uint64_t pb_topo_depth_unit_scratch(const pose_hbm_topo_t *t);
-int pb_topo_launch_depth(const pose_hbm_topo_t *t, const uint32_t *d_seeds, void *dev_ptr, uint64_t nsuper,
-                         uint8_t *scratch, uint32_t grid, unsigned int *d_queue, cudaStream_t stream);
-
 /* Passes a team of T warps makes over all levels running G units in lockstep. */
 uint64_t pb_topo_passes(const pose_hbm_topo_t *t, uint32_t T, uint32_t G);
 /* Free device memory usable for scratch under an optional cap (the topology's

@@ -116,10 +116,10 @@ def test_deep_requests_run_as_a_second_launch(pkg, cuda):
             t.free()
 
 
-@pytest.mark.parametrize("deep_cb,shallow_cb,units", [(4096, 256, "1"), (4096, 256, "2"), (4096, 256, "4"),
-                                                     (3000, 100, "4")])
+@pytest.mark.parametrize("deep_cb,shallow_cb,units", [(4096, 256, "1"), (4096, 256, "2"), (4096, 256, "3"),
+                                                     (4096, 256, "4"), (3000, 100, "4"), (3000, 100, "3")])
 def test_multi_unit_depth_kernel_writes_the_same_bytes(pkg, cuda, monkeypatch, deep_cb, shallow_cb, units):
-    """The deep part on the multi-unit depth kernel with 1, 2 or 4 units per
+    """The deep part on the multi-unit depth kernel with 1 to 4 units per
     CTA (a ragged last batch, levels wider than the staged slots, session
     seeds of several lengths) writes what single calls and the lockstep
     kernel write."""

@@ -24,12 +24,13 @@ def test_plain_2e17_every_super_chunk(pkg, cuda, wl):
     cb, n = c["chunk_blocks"], c["chunks"]
     buf = cuda.zeros(n * cb * 32, dtype=cuda.uint8, device="cuda")
     with pkg.Topology(cb) as topo:
-        for kernel in (3, 1):
+        # the depth kernel alone and with a cluster of 2 CTAs per copy, and the lockstep kernel
+        for kernel, cl in ((3, 1), (3, 2), (1, 0)):
             rc, st = topo.label(c["key"], buf.data_ptr(), n * cb * 32, c["rbo"],
-                                sched=pkg.Sched(kernel=kernel), stats=True)
+                                sched=pkg.Sched(kernel=kernel, cluster_ctas=cl), stats=True)
             assert rc == 0, pkg.last_error()
-            assert st["kernel"] == kernel
-            assert digests(cuda, buf, cb * 32, n) == g["super_chunk_sha256"], kernel
+            assert st["kernel"] == kernel and st["cluster_ctas"] == cl
+            assert digests(cuda, buf, cb * 32, n) == g["super_chunk_sha256"], (kernel, cl)
             buf.zero_()
         # the block-0 table and in-register block 0 give the same bytes
     with pkg.Topology(cb, cv0_table=False) as topo:
@@ -43,11 +44,14 @@ def test_deep_2e20_every_super_chunk_under_40GiB_cap(pkg, cuda, wl):
     cb, n = c["chunk_blocks"], c["chunks"]
     buf = cuda.zeros(n * cb * 32, dtype=cuda.uint8, device="cuda")
     with pkg.Topology(cb) as topo:
-        s = pkg.Sched(scratch_cap_bytes=c["scratch_cap_bytes"])
-        rc, st = topo.label(c["key"], buf.data_ptr(), n * cb * 32, c["rbo"], sched=s, stats=True)
-        assert rc == 0, pkg.last_error()
-        assert st["scratch_bytes"] <= c["scratch_cap_bytes"]
-    assert digests(cuda, buf, cb * 32, n) == g["super_chunk_sha256"]
+        # the automatic schedule, and the depth kernel with clusters of 8 CTAs per copy
+        for cl in (0, 8):
+            s = pkg.Sched(scratch_cap_bytes=c["scratch_cap_bytes"], cluster_ctas=cl, kernel=3 if cl else 0)
+            rc, st = topo.label(c["key"], buf.data_ptr(), n * cb * 32, c["rbo"], sched=s, stats=True)
+            assert rc == 0, pkg.last_error()
+            assert st["scratch_bytes"] <= c["scratch_cap_bytes"]
+            assert digests(cuda, buf, cb * 32, n) == g["super_chunk_sha256"], st
+            buf.zero_()
 
 
 def test_batched_sessions_sampled_chunks(pkg, cuda, wl):

@@ -99,6 +99,38 @@ def test_warp_specialised_kernel_gives_the_same_bytes(pkg, cuda, wl, oracle, nc)
         assert got == oracle.label_region(key, cb, 5, cb * 3, threads=8).tobytes(), cb
 
 
+@pytest.mark.parametrize("C,split", [(2, None), (4, None), (8, None), (2, "0"), (4, "100"), (8, "0")])
+def test_cluster_depth_kernel_gives_the_same_bytes(pkg, cuda, oracle, monkeypatch, C, split):
+    """The depth kernel with a cluster of C CTAs per chunk copy sharing the
+    levels wider than the split width: the default width, every level
+    shared (width 0), and a narrow width; power-of-two and other
+    chunk_blocks, unaligned positions."""
+    if split is not None:
+        monkeypatch.setenv("POSE_B200_SPLIT_WIDTH", split)  # read when the topology is built
+    rnd = random.Random(C * 31 + (int(split) if split else 7))
+    for cb, nsup in ((1024, 8), (4096, 4), (3000, 3)):
+        nsup = min(nsup, 16 // C)  # one wave of clusters: at most 8 C-CTA clusters of 2 copies
+        key = rnd.randbytes(32)
+        rbo = cb * rnd.randrange(1 << 20) + rnd.randrange(cb)
+        s = pkg.Sched(kernel=3, cluster_ctas=C)
+        buf = dev_buffer(cuda, nsup * cb * 32)
+        with pkg.Topology(cb) as topo:
+            rc, st = topo.label(key, buf.data_ptr(), nsup * cb * 32, rbo, sched=s, stats=True)
+        cuda.cuda.synchronize()
+        assert rc == 0, pkg.last_error()
+        assert st["kernel"] == 3 and st["cluster_ctas"] == C
+        assert host_bytes(buf) == oracle.label_region(key, cb, nsup, rbo, threads=8).tobytes(), (cb, C, split)
+
+
+def test_cluster_schedule_is_validated(pkg, cuda):
+    with pkg.Topology(1024) as topo:
+        buf = cuda.zeros(1024 * 32, dtype=cuda.uint8, device="cuda")
+        for bad in (pkg.Sched(kernel=1, cluster_ctas=2), pkg.Sched(kernel=3, cluster_ctas=3),
+                    pkg.Sched(kernel=3, cluster_ctas=32)):
+            assert topo.label(bytes(32), buf.data_ptr(), 1024 * 32, 0, sched=bad) == -1
+            assert "cluster_ctas" in pkg.last_error()
+
+
 def test_retired_kernel_number_is_refused(pkg, cuda):
     with pkg.Topology(1024) as topo:
         buf = cuda.zeros(1024 * 32, dtype=cuda.uint8, device="cuda")
@@ -188,8 +220,29 @@ def test_stats_report_the_work(pkg, cuda):
     buf = dev_buffer(cuda, 8 * 1024 * 32)
     with pkg.Topology(1024) as topo:
         rc, st = topo.label(b"s" * 32, buf.data_ptr(), 8 * 1024 * 32, 0, stats=True)
-        assert st["kernel"] in (1, 2, 3)
+        assert st["kernel"] in (1, 3)
     assert rc == 0
     assert st["super_chunks"] == 8 and st["units"] == 16
     assert st["nodes"] == 8 * 96254
     assert st["kernel_ms"] > 0 and st["kernel_launches"] == 1
+
+
+@pytest.mark.parametrize("team_warps,per_sm", [(16, 1), (1, 3), (4, 7)])
+def test_teams_per_sm_cap_keeps_the_bytes(pkg, cuda, oracle, team_warps, per_sm):
+    # k teams on every SM, held there by padding each CTA's shared memory:
+    # every SM gets the same number of teams, and the bytes do not change
+    import os
+    key, cb, nsup, rbo = b"\x5a" * 32, 64, 1200, 64 * 17
+    sms = cuda.cuda.get_device_properties(0).multi_processor_count
+    s = pkg.Sched(kernel=1, team_warps=team_warps, units_per_team=1)
+    os.environ["POSE_B200_TEAMS_PER_SM"] = str(per_sm)
+    try:
+        buf = dev_buffer(cuda, nsup * cb * 32)
+        with pkg.Topology(cb) as topo:
+            rc, st = topo.label(key, buf.data_ptr(), nsup * cb * 32, rbo, sched=s, stats=True)
+        cuda.cuda.synchronize()
+    finally:
+        os.environ.pop("POSE_B200_TEAMS_PER_SM", None)
+    assert rc == 0, pkg.last_error()
+    assert st["teams"] == per_sm * sms
+    assert host_bytes(buf) == oracle.label_region(key, cb, nsup, rbo, threads=8).tobytes()

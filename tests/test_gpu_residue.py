@@ -47,7 +47,7 @@ def test_workspace_is_clear_after_each_kind_of_call(pkg, cuda):
         assert topo.label(key, buf.data_ptr(), n, 0) == 0, pkg.last_error()
         assert cuda.count_nonzero(buf) > 0          # labels were written to the caller's buffer
         assert topo.residue() == 0                  # and nothing else stayed behind
-        for kernel in (1, 2, 3):
+        for kernel in (1, 3):
             sched = pkg.Sched(kernel=kernel)
             assert topo.label(key, buf.data_ptr(), n, 1024 * 5, sched=sched) == 0, pkg.last_error()
             assert topo.residue() == 0, f"kernel {kernel}"

@@ -66,16 +66,21 @@ def test_oversized_request_is_rejected(pkg, cuda):
         assert srv.submit(topo, 99, buf.data_ptr(), 4096 * 32, 0) == -1  # unknown session
 
 
-def test_deep_requests_run_on_the_depth_kernel_and_match_alone(pkg, cuda):
-    """Requests at chunk_blocks 2^17 run alone on the depth kernel while
-    shallow requests keep forming waves around them; every result equals
-    labelling that request alone."""
+@pytest.mark.parametrize("deep_sms", [0, 2])
+def test_deep_requests_run_on_the_depth_kernel_and_match_alone(pkg, cuda, monkeypatch, deep_sms):
+    """Requests at chunk_blocks 2^17 run on the multi-unit depth kernel while
+    shallow requests keep forming waves around them — one chunk copy per CTA
+    on an idle GPU, and with the depth kernel held to 2 SMs, four per CTA,
+    the CTAs looping over the batches, a ragged one last; every result
+    equals labelling that request alone."""
+    if deep_sms:
+        monkeypatch.setenv("POSE_B200_SERVER_DEEP_SMS", str(deep_sms))
     rnd = random.Random(17)
     deep_cb, cbs = 1 << 17, [1024, 1 << 14]
     topos = {cb: pkg.Topology(cb) for cb in [deep_cb] + cbs}
     try:
         seed_list = [rnd.randbytes(32) for _ in range(3)]
-        plan = [(deep_cb, 2), (1024, 3), (1 << 14, 2), (deep_cb, 3), (1024, 5), (1 << 14, 1), (1024, 2)]
+        plan = [(deep_cb, 2), (1024, 3), (1 << 14, 2), (deep_cb, 5), (1024, 5), (1 << 14, 1), (1024, 2)]
         reqs = []
         for cb, ns in plan:
             reqs.append((cb, ns, cb * rnd.randrange(1 << 16), rnd.randrange(3),

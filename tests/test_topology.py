@@ -275,3 +275,45 @@ def test_pipelined_records_are_safe(host, cb, csm):
         outbit = (r2[a:b, 0] >> 30) & 1
         assert ((r2[a:b, 5] != 0xFFFFFFFF) == (outbit == 1)).all()
     assert info["gpool2"] <= info["pool"]
+
+
+def cluster_barriers(lstart, split_width):
+    """The cluster-barrier sequences of the depth kernel's cluster form
+    (label_ws.cu, k_label_wsc), restated: rank 0 passes a cluster barrier at
+    boundary b (between levels b - 1 and b) when level b - 1 or b is wider
+    than split_width; the other ranks walk the split levels in order and
+    pass boundary l before split level l unless l - 1 was split too, and
+    boundary l + 1 after it."""
+    w = np.diff(np.asarray(lstart, dtype=np.int64))
+    L = len(w)
+    split = w > split_width
+    rank0 = [b for b in range(L + 1)
+             if (b > 0 and split[b - 1]) or (b < L and split[b])]
+    levels = [int(x) for x in np.nonzero(split)[0]]
+    helper = []
+    for k, l in enumerate(levels):
+        if k == 0 or levels[k - 1] + 1 != l:
+            helper.append(l)
+        helper.append(l + 1)
+    return rank0, helper
+
+
+@pytest.mark.parametrize("cb", [64, 1024, 3000, 4096, 1 << 14])
+def test_cluster_ranks_pass_the_same_barriers(host, cb):
+    """Every CTA of a depth-kernel cluster passes the same cluster barriers in
+    the same order (a rank that skipped or repeated one would leave the
+    others waiting), for the default split width and for the extremes."""
+    t = HostTopo()
+    assert host.pb_topo_host_build(cb, C.byref(t)) == 0
+    try:
+        lstart = np.ctypeslib.as_array(t.lstart, shape=(t.L + 1,)).copy()
+    finally:
+        host.pb_topo_host_free(C.byref(t))
+    for sw in (0, 1, 100, 480, 224, 1 << 30):
+        rank0, helper = cluster_barriers(lstart, sw)
+        assert rank0 == helper, (cb, sw)
+        assert helper == sorted(set(helper)), (cb, sw)
+        if sw == 0:
+            assert rank0 == list(range(len(lstart)))  # every boundary
+        if sw == 1 << 30:
+            assert rank0 == []
