@@ -319,7 +319,10 @@ static int make_plan(const pose_hbm_topo_t *ct, uint64_t nunits, const pose_b200
         uint64_t sbytes = nunits * team_scratch;
         if (sbytes > budget) continue;
         uint64_t passes = passes_lanes(t, 32ull * nc);
-        double lat = (double)t->L * model_ws_latency() + (double)(passes - t->L) * t_lat / C +
+        /* the cluster form runs every level ~250 clocks slower than the
+         * one-CTA kernel (measured at 2^17: 742 ms against 693 ms with only
+         * 169 shared levels), so it pays only where wide levels dominate */
+        double lat = (double)t->L * (model_ws_latency() + 250.0) + (double)(passes - t->L) * t_lat / C +
                      2.0 * t->nsplit * model_cluster_sync();
         double cost = lat;
         if (best->cost < 0 || cost < best->cost * 0.999) {

@@ -57,6 +57,10 @@
 #define PB_SERVER_DEEP_LEVELS 300000u
 /* Hashing warps of a depth-kernel CTA. */
 #define PB_SERVER_DEEP_WARPS 15u
+/* A deep request takes the depth kernel only while at most this many
+ * requests are pending: a longer queue means a loaded GPU, where the waves'
+ * lockstep kernel serves more copies per SM. */
+#define PB_SERVER_DEEP_QUEUE 4u
 
 typedef struct {
     const pose_hbm_topo_t *topo;
@@ -217,13 +221,14 @@ static int slot_reqs(wave_t *wv, size_t n)
 
 /* With the lock held: launch the pending deep requests of the oldest pending
  * deep request's topology, oldest first, on the multi-unit depth kernel in a
- * free deep slot.  G units per CTA, as few as the free SMs allow (a CTA per
- * SM at most: the CTAs in flight count against the SMs), so one CTA runs one
- * copy's chain on an idle GPU and four under load; the CTAs pull the
- * launch's batches from a queue.  Requests are taken while they fit four
- * units per free SM (the first always).  The requests complete with the
- * launch.  Returns 1 when something was launched (or failed), 0 when it has
- * to wait for a slot, SMs or scratch. */
+ * free deep slot, one chunk copy per CTA and CTA per SM (the CTAs in flight
+ * count against the SMs): the shortest chains.  Requests are taken while
+ * their copies fit the free SMs.  When the oldest one does not fit, or more
+ * than PB_SERVER_DEEP_QUEUE requests are pending, the GPU is loaded: it joins
+ * the next wave instead, where the lockstep kernel packs many copies per SM
+ * (on a loaded GPU the depth kernel's one SM per copy costs more throughput
+ * than its shorter chain saves).  The requests complete with the launch.  Returns 1 when something was launched, failed
+ * or moved to the waves, 0 when nothing could be done. */
 static int admit_deep(pose_b200_server_t *s)
 {
     size_t i0 = s->next_pending;
@@ -231,20 +236,26 @@ static int admit_deep(pose_b200_server_t *s)
     if (i0 >= s->nreqs) return 0;
     int w = -1;
     for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP && w < 0; i++) if (!s->deeps[i].busy) w = (int)i;
-    if (w < 0 || s->deep_ctas >= s->sms) return 0;
     const pose_hbm_topo_t *topo = s->reqs[i0].topo;
     pb_topo_internal_t ti;
     pb_topo_view2_t v2;
     if (pb_topo_internal(topo, &ti) != 0 || pb_topo_view2_small(topo, &v2) != 0) return 0;
-    const uint32_t free_sms = s->sms - s->deep_ctas;
-    /* the group: same topology, oldest first, while four units per free SM hold them */
+    const uint32_t free_sms = s->deep_ctas < s->sms ? s->sms - s->deep_ctas : 0;
+    const uint64_t units0 = (s->reqs[i0].len / ti.super_bytes) * ti.copies;
+    size_t pending = 0;
+    for (size_t i = s->next_pending; i < s->nreqs; i++) pending += s->reqs[i].state == 0;
+    if (w < 0 || units0 > free_sms || pending > PB_SERVER_DEEP_QUEUE) {
+        s->reqs[i0].deep = 0; /* to the waves */
+        return 1;
+    }
+    /* the group: same topology, oldest first, while its copies fit the free SMs */
     size_t n = 0;
     uint64_t units = 0, nsuper = 0;
     for (size_t i = i0; i < s->nreqs; i++) {
         const sreq_t *r = &s->reqs[i];
         if (r->state != 0 || !r->deep || r->topo != topo) continue;
         const uint64_t ns = r->len / ti.super_bytes;
-        if (n > 0 && units + ns * ti.copies > 4ull * free_sms) break;
+        if (n > 0 && units + ns * ti.copies > free_sms) break;
         units += ns * ti.copies;
         nsuper += ns;
         n++;
@@ -268,17 +279,8 @@ static int admit_deep(pose_b200_server_t *s)
         pthread_cond_broadcast(&s->cv);
         return 1;
     }
-    /* an idle depth kernel runs the group at the fewest units per CTA that
-     * fit the free SMs (the shortest chains); while other depth work runs or
-     * waits, four per CTA (the most chains per SM: four units' narrow levels
-     * still take one warp pass) */
-    size_t pending_deep = 0;
-    for (size_t i = i0; i < s->nreqs; i++) pending_deep += s->reqs[i].state == 0 && s->reqs[i].deep;
-    const int more = s->deep_ctas > 0 || pending_deep > n;
-    uint32_t G = more ? 4u : (uint32_t)((units + free_sms - 1) / free_sms);
-    if (G < 1) G = 1;
-    if (G > 4) G = 4;
-    const uint64_t nbatches = (units + G - 1) / G;
+    const uint32_t G = 1;
+    const uint64_t nbatches = units;
     uint32_t grid = (uint32_t)(nbatches < free_sms ? nbatches : free_sms);
     const uint64_t per = (uint64_t)v2.gpool * 32 * G;
     const uint64_t fit = arena_largest(s) / per;
@@ -674,7 +676,8 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
         uint32_t mx = 0;
         if (pb_dev_label_wsg_prepare(&mx) != 0) mx = 0; /* no depth kernel: deep requests join waves */
         cudaGetLastError();
-        s->wsg_smem_max = mx;
+        const char *ed = getenv("POSE_B200_SERVER_DEEP"); /* 0: every request joins the waves */
+        s->wsg_smem_max = ed && ed[0] == '0' ? 0 : mx;
     }
     if (pb_dev_label_multi_occupancy(256, &s->occ) != 0) s->occ = 1;
     s->running = 1;

@@ -66,13 +66,13 @@ def test_oversized_request_is_rejected(pkg, cuda):
         assert srv.submit(topo, 99, buf.data_ptr(), 4096 * 32, 0) == -1  # unknown session
 
 
-@pytest.mark.parametrize("deep_sms", [0, 2])
+@pytest.mark.parametrize("deep_sms", [0, 8])
 def test_deep_requests_run_on_the_depth_kernel_and_match_alone(pkg, cuda, monkeypatch, deep_sms):
-    """Requests at chunk_blocks 2^17 run on the multi-unit depth kernel while
-    shallow requests keep forming waves around them — one chunk copy per CTA
-    on an idle GPU, and with the depth kernel held to 2 SMs, four per CTA,
-    the CTAs looping over the batches, a ragged one last; every result
-    equals labelling that request alone."""
+    """A request at chunk_blocks 2^17 on an idle GPU runs on the depth
+    kernel, one chunk copy per CTA; deep requests that arrive with a queue,
+    or (with the depth kernel held to 8 SMs) do not fit the free SMs, join
+    the waves of shallow requests.  Every result equals labelling that
+    request alone."""
     if deep_sms:
         monkeypatch.setenv("POSE_B200_SERVER_DEEP_SMS", str(deep_sms))
     rnd = random.Random(17)
@@ -88,8 +88,15 @@ def test_deep_requests_run_on_the_depth_kernel_and_match_alone(pkg, cuda, monkey
         cuda.cuda.synchronize()
         with pkg.Server(scratch_bytes=2 << 30, max_waves=2) as srv:
             sessions = [srv.session(k) for k in seed_list]
-            tickets = [srv.submit(topos[cb], sessions[sid], buf.data_ptr(), ns * cb * 32, rbo)
-                       for cb, ns, rbo, sid, buf in reqs]
+            for t in topos.values():
+                srv.prepare(t)
+            # the first deep request alone (an idle GPU: the depth kernel), then
+            # the rest in a burst (deep requests that find a queue join waves)
+            cb, ns, rbo, sid, buf = reqs[0]
+            first = srv.submit(topos[cb], sessions[sid], buf.data_ptr(), ns * cb * 32, rbo)
+            assert srv.wait(first)[0] == 0
+            tickets = [first] + [srv.submit(topos[cb], sessions[sid], buf.data_ptr(), ns * cb * 32, rbo)
+                                 for cb, ns, rbo, sid, buf in reqs[1:]]
             assert all(t >= 0 for t in tickets)
             for t in tickets:
                 rc, q, tot = srv.wait(t)
