@@ -349,11 +349,12 @@ static size_t split_deep(const pb_req_t *pr, size_t n, uint8_t *deep)
 }
 
 /* Size, allocate and upload one launch of a batch; `slots` caps its resident
- * CTAs and `budget` its scratch.  Returns 0, or -1 (message on stderr). */
+ * threads in units of 256 (256 / 32T teams each) and `budget` its scratch.
+ * One team per CTA.  Returns 0, or -1 (message on stderr). */
 static int part_setup(pose_b200_batch_t *b, batch_part_t *q, const pb_plan_tables_t *pl, uint32_t T,
                       uint64_t slots, uint64_t budget, const pose_b200_sched_t *sched)
 {
-    const uint32_t cta = 256, tpc = cta / (32 * T);
+    const uint32_t tpc = 256 / (32 * T);
     q->T = T;
     q->nbatches = pl->nbatches;
     q->njobs = pl->njobs;
@@ -373,11 +374,8 @@ static int part_setup(pose_b200_batch_t *b, batch_part_t *q, const pb_plan_table
                 (unsigned long long)pl->team_scratch);
         return -1;
     }
-    /* CTAs of up to tpc teams; every team of every CTA has its scratch */
-    const uint32_t ctpc = R < tpc ? (uint32_t)R : tpc;
-    q->grid = (uint32_t)(R / ctpc);
-    R = (uint64_t)q->grid * ctpc;
-    q->cta_threads = 32 * T * ctpc;
+    q->grid = (uint32_t)R;
+    q->cta_threads = 32 * T;
     q->teams = (uint32_t)R;
     q->fma = (double)R * T / pl->sms >= 8.0;
     q->scratch_bytes = R * pl->team_scratch;

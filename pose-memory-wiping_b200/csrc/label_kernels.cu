@@ -321,30 +321,30 @@ __global__ void __launch_bounds__(PB_CTA_THREADS) k_label(const __grid_constant_
 
 /* Many topologies in one launch: teams take batches (same topology, up to
  * G = 2^glog units) from a queue sorted longest first, and copy the batch's
- * topology view into shared memory. */
+ * topology view into shared memory.  One team of T warps per CTA
+ * (blockDim.x == 32 T), ending its levels with the CTA barrier. */
 template <bool FMA>
 __global__ void __launch_bounds__(PB_MULTI_CTA_THREADS, 3) k_label_multi(const __grid_constant__ pb_multi_params_t p)
 {
     const uint32_t T = p.team_warps;
     const uint32_t TT = T * 32;
-    const uint32_t team = (threadIdx.x >> 5) / T;
-    const uint32_t tt = threadIdx.x - team * TT;
-    const uint32_t teams_per_cta = blockDim.x / TT;
-    const uint64_t gteam = (uint64_t)blockIdx.x * teams_per_cta + team;
-    const uint32_t bar_id = 1 + team;
-    __shared__ uint32_t s_batch[PB_CTA_THREADS / 32];
-    __shared__ pb_topo_view_t s_topo[PB_CTA_THREADS / 32];
+    const uint32_t team = 0;
+    const uint32_t tt = threadIdx.x;
+    const uint64_t gteam = blockIdx.x;
+    const uint32_t bar_id = 0;
+    __shared__ uint32_t s_batch[1];
+    __shared__ pb_topo_view_t s_topo[1];
     UnitCtx c;
     c.tscr = reinterpret_cast<uint4 *>(p.scratch + gteam * p.team_scratch_bytes);
 
     for (;;) {
-        const uint32_t batch = grab_batch<false>(p.queue, T, team, tt, bar_id, TT, s_batch);
+        const uint32_t batch = grab_batch<true>(p.queue, T, team, tt, bar_id, TT, s_batch);
         if (batch >= p.nbatches) break;
         const pb_mbatch_t bd = p.batches[batch];
         if (tt < sizeof(pb_topo_view_t) / 4)
             reinterpret_cast<uint32_t *>(&s_topo[team])[tt] =
                 reinterpret_cast<const uint32_t *>(p.topos + bd.topo)[tt];
-        team_sync<false>(T, bar_id, TT);
+        team_sync<true>(T, bar_id, TT);
         const pb_topo_view_t &tp = s_topo[team];
         c.glog = bd.glog;
         c.u = tt & ((1u << c.glog) - 1);
@@ -360,14 +360,14 @@ __global__ void __launch_bounds__(PB_MULTI_CTA_THREADS, 3) k_label_multi(const _
         c.cv0 = tp.cv0 ? tp.cv0 + (uint64_t)copy * tp.S * 2 : nullptr;
 #pragma unroll
         for (int i = 0; i < 8; i++) c.seed[i] = c.valid ? p.seeds[8 * (size_t)un.seed + i] : 0u;
-        label_levels<FMA, false>(tp, c, T, bar_id, TT, p.one);
+        label_levels<FMA, true>(tp, c, T, bar_id, TT, p.one);
         /* label_levels ended with a team barrier, so every persisted label of
          * the batch is ordered before this fence */
         if (p.req_done != nullptr && tt < bd.count) {
             __threadfence_system();
             atomicAdd_system(p.req_done + p.unit_req[bd.first_unit + tt], 1u);
         }
-        team_sync<false>(T, bar_id, TT); /* s_topo[team] is rewritten by the next batch */
+        team_sync<true>(T, bar_id, TT); /* s_topo[team] is rewritten by the next batch */
     }
 }
 
@@ -561,7 +561,7 @@ extern "C" int pb_dev_label(const pb_label_params_t *params, uint32_t grid, uint
 extern "C" int pb_dev_label_multi(const pb_multi_params_t *params, uint32_t grid, uint32_t cta_threads,
                                   cudaStream_t stream)
 {
-    if (cta_threads == 0 || cta_threads > PB_MULTI_CTA_THREADS) return -1;
+    if (cta_threads != 32u * params->team_warps || cta_threads > PB_MULTI_CTA_THREADS) return -1; /* one team per CTA */
     cudaGetLastError(); /* report only this launch */
     const uint32_t smem = PB_PREF_BYTES_PER_THREAD * cta_threads;
     if (params->fma_adds) pb::k_label_multi<true><<<grid, cta_threads, smem, stream>>>(*params);

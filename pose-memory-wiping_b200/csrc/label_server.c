@@ -438,16 +438,14 @@ static int admit_wave(pose_b200_server_t *s)
         return 1;
     }
     /* teams: as many as fit in the largest free arena range, the GPU and the
-     * batches; CTAs of up to 256 threads, every team with its scratch */
+     * batches; one team per CTA, every team with its scratch */
     const uint32_t tpc_max = 256 / (32 * Tw);
     uint64_t cap = (uint64_t)pl.sms * (s->occ > 0 ? s->occ : 1) * tpc_max;
     uint64_t R = arena_largest(s) / pl.team_scratch;
     if (R > cap) R = cap;
     if (R > pl.nbatches) R = pl.nbatches;
     if (R == 0) { pb_plan_free(&pl); return 0; } /* wait for scratch to free up */
-    const uint32_t tpc = R < tpc_max ? (uint32_t)R : tpc_max;
-    const uint32_t g2 = (uint32_t)(R / tpc);
-    R = (uint64_t)g2 * tpc;
+    const uint32_t g2 = (uint32_t)R; /* one team per CTA */
     const uint64_t scratch = R * pl.team_scratch;
     uint64_t off = 0;
     if (arena_take(s, scratch, &off) != 0) { pb_plan_free(&pl); return 0; }
@@ -508,7 +506,7 @@ static int admit_wave(pose_b200_server_t *s)
     p.one = 1;
     p.unit_req = (const uint32_t *)(T + o_ureq);
     p.req_done = wv->d_done;
-    if (ok) ok = pb_dev_label_multi(&p, g2, 32 * Tw * tpc, wv->stream) == 0;
+    if (ok) ok = pb_dev_label_multi(&p, g2, 32 * Tw, wv->stream) == 0;
     /* the scratch range and the chunk seeds are zeroed before the wave
      * counts as done */
     if (ok) ok = cudaMemsetAsync(s->d_arena + off, 0, scratch, wv->stream) == cudaSuccess;
