@@ -284,8 +284,9 @@ int pose_b200_verify_sampled(const pose_hbm_topo_t *topo, const uint8_t *session
  * callers that must not call cudaMalloc while they label — e.g. a wipe worker
  * that reserved the device's free memory for its label window before
  * starting (a late allocation could fail half-way through a disk), or a host
- * whose own allocator or an active stream capture forbids new device
- * allocations.  The topology, seed and output buffer are still the caller's.
+ * whose own allocator already holds the device's memory and forbids new
+ * device allocations.  The topology, seed and output buffer are still the
+ * caller's.
  *
  * Its scratch pool (64 MiB), chunk-seed table (8192 seeds) and work counter
  * are static device arrays inside the library: a device holds them from when

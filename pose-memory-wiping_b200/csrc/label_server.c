@@ -51,7 +51,7 @@
 
 #define PB_SERVER_MAX_WAVES 16
 /* Concurrent launches of the depth kernel. */
-#define PB_SERVER_MAX_DEEP 16
+#define PB_SERVER_MAX_DEEP 64
 /* Requests whose topology has at least this many levels (chunk_blocks 2^17
  * and up) run on the depth kernel instead of joining a wave. */
 #define PB_SERVER_DEEP_LEVELS 300000u
@@ -112,6 +112,12 @@ struct pose_b200_server {
     wave_t deeps[PB_SERVER_MAX_DEEP]; /* depth-kernel launches, high-priority streams */
     uint32_t max_waves;        /* concurrent multi-topology waves */
     uint32_t deep_ctas;        /* depth-kernel CTAs in flight */
+    uint32_t deep_queue;       /* deep requests take the depth kernel while at most this many requests wait */
+    uint32_t deep_units;       /* units per depth CTA: 0 = the fewest of 1, 2, 4 that fit the free SMs */
+    uint32_t deep_gmax;        /* most units per depth CTA */
+    int deep_wait;             /* a deep request that does not fit waits for SMs instead of joining a wave */
+    int deep_excl;             /* a depth CTA holds its SM alone (shared memory raised to the limit) */
+    uint32_t deep_levels;      /* requests of topologies with at least this many levels are deep */
     uint32_t sms;
     uint32_t wsg_smem_max;     /* the depth kernel's shared-memory limit (0: no depth kernel) */
     int occ;
@@ -183,7 +189,7 @@ static int req_is_deep(const pose_b200_server_t *s, const pose_hbm_topo_t *topo)
 {
     pb_topo_internal_t ti;
     pb_topo_view2_t v2;
-    if (!s->wsg_smem_max || pb_topo_internal(topo, &ti) != 0 || ti.view.L < PB_SERVER_DEEP_LEVELS) return 0;
+    if (!s->wsg_smem_max || pb_topo_internal(topo, &ti) != 0 || ti.view.L < s->deep_levels) return 0;
     if (pb_topo_view2_small(topo, &v2) != 0) {
         cudaGetLastError();
         return 0;
@@ -244,18 +250,22 @@ static int admit_deep(pose_b200_server_t *s)
     const uint64_t units0 = (s->reqs[i0].len / ti.super_bytes) * ti.copies;
     size_t pending = 0;
     for (size_t i = s->next_pending; i < s->nreqs; i++) pending += s->reqs[i].state == 0;
-    if (w < 0 || units0 > free_sms || pending > PB_SERVER_DEEP_QUEUE) {
+    const uint32_t gmax = s->deep_units ? s->deep_units : s->deep_gmax;
+    uint64_t ctas0 = (units0 + gmax - 1) / gmax;
+    if (ctas0 > s->sms) ctas0 = s->sms; /* larger than the GPU: its CTAs loop over the batches */
+    if (pending > s->deep_queue || (!s->deep_wait && (w < 0 || ctas0 > free_sms))) {
         s->reqs[i0].deep = 0; /* to the waves */
         return 1;
     }
-    /* the group: same topology, oldest first, while its copies fit the free SMs */
+    if (w < 0 || ctas0 > free_sms) return 0; /* waits for a slot or SMs */
+    /* the group: same topology, oldest first, while its CTAs fit the free SMs */
     size_t n = 0;
     uint64_t units = 0, nsuper = 0;
     for (size_t i = i0; i < s->nreqs; i++) {
         const sreq_t *r = &s->reqs[i];
         if (r->state != 0 || !r->deep || r->topo != topo) continue;
         const uint64_t ns = r->len / ti.super_bytes;
-        if (n > 0 && units + ns * ti.copies > free_sms) break;
+        if (n > 0 && (units + ns * ti.copies + gmax - 1) / gmax > free_sms) break;
         units += ns * ti.copies;
         nsuper += ns;
         n++;
@@ -279,8 +289,14 @@ static int admit_deep(pose_b200_server_t *s)
         pthread_cond_broadcast(&s->cv);
         return 1;
     }
-    const uint32_t G = 1;
-    const uint64_t nbatches = units;
+    /* units per CTA: the fewest that fit the free SMs (the shortest chains) */
+    uint32_t G = s->deep_units;
+    if (!G) {
+        G = 1;
+        while (G < gmax && (units + G - 1) / G > free_sms) G *= 2;
+        if (G > gmax) G = gmax;
+    }
+    const uint64_t nbatches = (units + G - 1) / G;
     uint32_t grid = (uint32_t)(nbatches < free_sms ? nbatches : free_sms);
     const uint64_t per = (uint64_t)v2.gpool * 32 * G;
     const uint64_t fit = arena_largest(s) / per;
@@ -344,8 +360,9 @@ static int admit_deep(pose_b200_server_t *s)
         p.team_warps = PB_SERVER_DEEP_WARPS;
         p.nbatches = (uint32_t)nbatches;
         p.queue = (unsigned int *)(T + o_queue);
+        const uint32_t need = pb_wsg_smem_bytes(v2.csm, G, PB_SERVER_DEEP_WARPS);
         ok = pb_dev_label_wsg(&p, grid, 32 * (PB_SERVER_DEEP_WARPS + 1),
-                              pb_wsg_smem_bytes(v2.csm, G, PB_SERVER_DEEP_WARPS), wv->stream) == 0;
+                              s->deep_excl && s->wsg_smem_max > need ? s->wsg_smem_max : need, wv->stream) == 0;
     }
     /* scratch and chunk seeds are zeroed before the requests count as done */
     ok = ok && cudaMemsetAsync(s->d_arena + off, 0, scratch, wv->stream) == cudaSuccess;
@@ -676,8 +693,47 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
         cudaGetLastError();
         const char *ed = getenv("POSE_B200_SERVER_DEEP"); /* 0: every request joins the waves */
         s->wsg_smem_max = ed && ed[0] == '0' ? 0 : mx;
+        /* deep-request policy (tuning): queue threshold, units per CTA, wait or join a wave, SM held alone */
+        s->deep_queue = PB_SERVER_DEEP_QUEUE;
+        s->deep_units = 0;
+        s->deep_gmax = 4;
+        s->deep_wait = 0;
+        s->deep_excl = 0;
+        s->deep_levels = PB_SERVER_DEEP_LEVELS;
+        const char *e0 = getenv("POSE_B200_SERVER_DEEP_LEVELS");
+        if (e0 && atoi(e0) > 0) s->deep_levels = (uint32_t)atoi(e0);
+        const char *e1 = getenv("POSE_B200_SERVER_DEEP_QUEUE");
+        if (e1 && e1[0]) s->deep_queue = (uint32_t)atoi(e1);
+        const char *e2 = getenv("POSE_B200_SERVER_DEEP_UNITS");
+        if (e2 && atoi(e2) >= 1 && atoi(e2) <= 4) s->deep_units = (uint32_t)atoi(e2);
+        const char *e3 = getenv("POSE_B200_SERVER_DEEP_GMAX");
+        if (e3 && atoi(e3) >= 1 && atoi(e3) <= 4) s->deep_gmax = (uint32_t)atoi(e3);
+        const char *e4 = getenv("POSE_B200_SERVER_DEEP_WAIT");
+        if (e4 && e4[0]) s->deep_wait = atoi(e4) != 0;
+        const char *e5 = getenv("POSE_B200_SERVER_DEEP_EXCL");
+        if (e5 && e5[0]) s->deep_excl = atoi(e5) != 0;
     }
     if (pb_dev_label_multi_occupancy(256, &s->occ) != 0) s->occ = 1;
+    /* Launch tables and completion counters of every slot, allocated up
+     * front: the dispatcher then makes no allocation while kernels run (a
+     * cudaFree there waits for the whole device, and the submitters and
+     * waiters wait on the dispatcher's lock meanwhile).  Best effort: a slot
+     * whose buffers could not be had grows them on first use. */
+    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
+        wave_t *wv = &s->waves[i];
+        if (slot_tables(wv, (size_t)512 << 10) != 0) cudaGetLastError();
+        if (cudaHostAlloc((void **)&wv->h_done, 4096 * sizeof(unsigned int), cudaHostAllocMapped) == cudaSuccess &&
+            cudaHostGetDevicePointer((void **)&wv->d_done, wv->h_done, 0) == cudaSuccess) {
+            wv->done_cap = 4096;
+        } else {
+            if (wv->h_done) cudaFreeHost(wv->h_done);
+            wv->h_done = NULL;
+            wv->d_done = NULL;
+            cudaGetLastError();
+        }
+    }
+    for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP; i++)
+        if (slot_tables(&s->deeps[i], (size_t)64 << 10) != 0) cudaGetLastError();
     s->running = 1;
     if (pthread_create(&s->thread, NULL, dispatcher, s) != 0) { s->running = 0; goto fail; }
     return s;
@@ -686,10 +742,13 @@ fail:
     for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
         if (s->waves[i].stream) cudaStreamDestroy(s->waves[i].stream);
         if (s->waves[i].done) cudaEventDestroy(s->waves[i].done);
+        cudaFree(s->waves[i].d_tables);
+        if (s->waves[i].h_done) cudaFreeHost(s->waves[i].h_done);
     }
     for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP; i++) {
         if (s->deeps[i].stream) cudaStreamDestroy(s->deeps[i].stream);
         if (s->deeps[i].done) cudaEventDestroy(s->deeps[i].done);
+        cudaFree(s->deeps[i].d_tables);
     }
     cudaFree(s->d_arena);
     pthread_mutex_destroy(&s->mu);
@@ -759,6 +818,7 @@ int64_t pose_b200_server_submit(pose_b200_server_t *s, const pose_hbm_topo_t *to
                                 size_t len, uint64_t region_block_offset)
 {
     if (!s || !topo) return -1;
+    const double t_submit = now_ms(); /* latency counts from the call, lock wait included */
     /* before the lock: a deep topology's first request builds its records */
     const int deep = req_is_deep(s, topo);
     pthread_mutex_lock(&s->mu);
@@ -798,7 +858,7 @@ int64_t pose_b200_server_submit(pose_b200_server_t *s, const pose_hbm_topo_t *to
     r->rbo = region_block_offset;
     r->session = session;
     r->deep = deep;
-    r->t_submit = now_ms();
+    r->t_submit = t_submit;
     id = (int64_t)s->nreqs++;
     pthread_cond_broadcast(&s->cv);
 out:
