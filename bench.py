@@ -37,6 +37,10 @@ import subprocess
 import sys
 import time
 
+# One host-to-device work queue per server slot (the default is 8 queues,
+# shared by the server's streams); read when CUDA initialises, so set here.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(ROOT, "pose-memory-wiping_b200")
 MIB = float(1 << 20)

@@ -640,10 +640,6 @@ no_split:
         if (pl[0].nunits == 0 && !nd) { fprintf(stderr, "pose_b200_batch_create: no super-chunk to label\n"); goto fail; }
         slots = (uint64_t)pl[0].sms * occ;
         slots = slots > b->part[1].grid ? slots - b->part[1].grid : 1;
-        {
-            const char *es = getenv("POSE_B200_SHALLOW_SLOTS_PCT"); /* tuning: scale the rest's team slots */
-            if (es && atoi(es) > 0 && atoi(es) < 100) slots = slots * (uint64_t)atoi(es) / 100 ? slots * (uint64_t)atoi(es) / 100 : 1;
-        }
         if (pl[0].nunits) {
             if (part_setup(b, &b->part[0], &pl[0], T, slots, budget, sched) != 0) goto fail;
         }

@@ -22,18 +22,24 @@
  *   - finished waves are reaped and their arena range is zeroed on the device
  *     before it is reused;
  *   - deep requests (topologies of at least PB_SERVER_DEEP_LEVELS levels,
- *     chunk_blocks 2^17 and up) do not join waves: the pending deep requests
+ *     chunk_blocks 2^18 and up) do not join waves: the pending deep requests
  *     of one topology run together on the multi-unit depth kernel
- *     (k_label_wsg: a producer warp and 15 hashing warps per CTA, 1 to 4
- *     chunk copies per CTA) in a slot of their own, on a high-priority
- *     stream, so a wave never waits for a deep chain and a deep chain never
- *     runs on the lockstep kernel.  At most one depth CTA per SM is in
- *     flight; the units per CTA grow with the load (as few as the free SMs
- *     allow: one per CTA on an idle GPU, for the shortest chain; four under
- *     load, for the most chains per SM).  Their scratch comes from the same
- *     arena;
- *   - admission never waits in line: a deep request that has to wait for
- *     SMs or scratch does not hold back the shallow requests behind it.
+ *     (k_label_wsg: a producer warp and 15 hashing warps per CTA, four chunk
+ *     copies per CTA) in a slot of their own, on a high-priority stream.
+ *     Each depth CTA holds its SM alone (its shared memory is raised to the
+ *     limit), so no lockstep warp slows its chain, and at most one depth CTA
+ *     per SM is in flight: a deep request that does not fit the free SMs
+ *     waits for them, without holding back the shallow requests behind it.
+ *     Their scratch comes from the same arena;
+ *   - the dispatcher never waits for the GPU: launch tables go up from
+ *     pinned per-slot staging, and every slot's buffers are allocated when
+ *     the server is created (an allocation, or a copy from pageable memory,
+ *     can wait behind the kernels already running);
+ *   - streams share the device's host-to-device work queues
+ *     (CUDA_DEVICE_MAX_CONNECTIONS, 8 unless the environment raises it), and
+ *     a stream's work that waits behind its own long kernel holds back every
+ *     other stream of the same queue; a launch takes a slot whose queue no
+ *     running launch uses.  With 32 queues every slot has its own.
  * Every request's bytes are those of labelling it alone.
  */
 #include "batch_internal.h"
@@ -51,16 +57,20 @@
 
 #define PB_SERVER_MAX_WAVES 16
 /* Concurrent launches of the depth kernel. */
-#define PB_SERVER_MAX_DEEP 64
-/* Requests whose topology has at least this many levels (chunk_blocks 2^17
- * and up) run on the depth kernel instead of joining a wave. */
-#define PB_SERVER_DEEP_LEVELS 300000u
+#define PB_SERVER_MAX_DEEP 16
+/* Requests whose topology has at least this many levels (chunk_blocks 2^18
+ * and up: a chunk copy's chain alone is 2.4 s on the lockstep kernel) run on
+ * the depth kernel instead of joining a wave.  On the 120-request Poisson
+ * trace (200 requests/s, chunk_blocks 2^10..2^18) this served 534 MiB/s,
+ * against 486 with 2^17 included (one SM per CTA holds more SM time than
+ * the lockstep kernel's 2^17 chains cost) and 448 with every request in
+ * waves. */
+#define PB_SERVER_DEEP_LEVELS 600000u
 /* Hashing warps of a depth-kernel CTA. */
 #define PB_SERVER_DEEP_WARPS 15u
-/* A deep request takes the depth kernel only while at most this many
- * requests are pending: a longer queue means a loaded GPU, where the waves'
- * lockstep kernel serves more copies per SM. */
-#define PB_SERVER_DEEP_QUEUE 4u
+/* A deep request joins a wave instead when more than this many requests
+ * are pending (tuning; by default never). */
+#define PB_SERVER_DEEP_QUEUE 0xffffffffu
 
 typedef struct {
     const pose_hbm_topo_t *topo;
@@ -80,6 +90,8 @@ typedef struct {
     uint64_t arena_off, arena_len;
     void *d_tables;
     size_t tables_cap;
+    uint8_t *h_stage;          /* pinned host copy of the launch tables, the uploads' source */
+    size_t stage_cap;
     uint64_t *reqs;
     uint32_t *need;            /* chunk copies of each request of the wave */
     size_t nreqs, reqs_cap;
@@ -87,6 +99,7 @@ typedef struct {
     unsigned int *d_done;
     size_t done_cap;
     int deep;                  /* deep requests on the depth kernel (complete with the launch) */
+    uint32_t chan;             /* the host-to-device work queue its stream maps to (creation order) */
     uint32_t ctas;             /* its CTAs, one SM each */
 } wave_t;
 
@@ -119,6 +132,7 @@ struct pose_b200_server {
     int deep_excl;             /* a depth CTA holds its SM alone (shared memory raised to the limit) */
     uint32_t deep_levels;      /* requests of topologies with at least this many levels are deep */
     uint32_t sms;
+    uint32_t conns;            /* host-to-device work queues (CUDA_DEVICE_MAX_CONNECTIONS, default 8) */
     uint32_t wsg_smem_max;     /* the depth kernel's shared-memory limit (0: no depth kernel) */
     int occ;
     uint64_t waves_launched;
@@ -213,6 +227,24 @@ static int slot_tables(wave_t *wv, size_t total)
     return 0;
 }
 
+/* Pinned host staging of one launch's tables, grown on demand.  The uploads
+ * from it are asynchronous, so the dispatcher never waits for the GPU: the
+ * slot's staging stays untouched until the slot is reaped. */
+static int slot_stage(wave_t *wv, size_t total)
+{
+    if (wv->stage_cap >= total) return 0;
+    if (wv->h_stage) cudaFreeHost(wv->h_stage);
+    wv->h_stage = NULL;
+    wv->stage_cap = 0;
+    if (cudaHostAlloc((void **)&wv->h_stage, total * 2, cudaHostAllocDefault) != cudaSuccess) {
+        wv->h_stage = NULL;
+        cudaGetLastError();
+        return -1;
+    }
+    wv->stage_cap = total * 2;
+    return 0;
+}
+
 static int slot_reqs(wave_t *wv, size_t n)
 {
     if (wv->reqs_cap >= n) return 0;
@@ -222,6 +254,19 @@ static int slot_reqs(wave_t *wv, size_t n)
     if (nn) wv->need = nn;
     if (!nr || !nn) return -1;
     wv->reqs_cap = n;
+    return 0;
+}
+
+/* Streams share the device's host-to-device work queues, assigned in
+ * creation order; work that waits behind a long kernel in one stream holds
+ * back every stream of its queue.  A launch therefore takes a free slot whose
+ * queue no busy slot uses. */
+static int chan_busy(const pose_b200_server_t *s, uint32_t chan)
+{
+    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++)
+        if (s->waves[i].busy && s->waves[i].chan == chan) return 1;
+    for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP; i++)
+        if (s->deeps[i].busy && s->deeps[i].chan == chan) return 1;
     return 0;
 }
 
@@ -241,7 +286,8 @@ static int admit_deep(pose_b200_server_t *s)
     while (i0 < s->nreqs && !(s->reqs[i0].state == 0 && s->reqs[i0].deep)) i0++;
     if (i0 >= s->nreqs) return 0;
     int w = -1;
-    for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP && w < 0; i++) if (!s->deeps[i].busy) w = (int)i;
+    for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP && w < 0; i++)
+        if (!s->deeps[i].busy && !chan_busy(s, s->deeps[i].chan)) w = (int)i;
     const pose_hbm_topo_t *topo = s->reqs[i0].topo;
     pb_topo_internal_t ti;
     pb_topo_view2_t v2;
@@ -289,12 +335,25 @@ static int admit_deep(pose_b200_server_t *s)
         pthread_cond_broadcast(&s->cv);
         return 1;
     }
-    /* units per CTA: the fewest that fit the free SMs (the shortest chains) */
+    /* units per CTA: on an otherwise idle depth kernel (nothing of it in
+     * flight, no other deep request waiting) the fewest that fit the free
+     * SMs, for the shortest chains; under load the most, for the most chains
+     * per SM (a narrow level of G units is still one warp pass) */
     uint32_t G = s->deep_units;
     if (!G) {
-        G = 1;
-        while (G < gmax && (units + G - 1) / G > free_sms) G *= 2;
-        if (G > gmax) G = gmax;
+        size_t others = 0;
+        for (size_t i = i0; i < s->nreqs; i++) {
+            const sreq_t *r = &s->reqs[i];
+            others += r->state == 0 && r->deep;
+        }
+        others -= n;
+        if (s->deep_ctas > 0 || others > 0) {
+            G = gmax;
+        } else {
+            G = 1;
+            while (G < gmax && (units + G - 1) / G > free_sms) G *= 2;
+            if (G > gmax) G = gmax;
+        }
     }
     const uint64_t nbatches = (units + G - 1) / G;
     uint32_t grid = (uint32_t)(nbatches < free_sms ? nbatches : free_sms);
@@ -311,14 +370,12 @@ static int admit_deep(pose_b200_server_t *s)
     const size_t o_seeds = AL(o_jobs + nsuper * sizeof(pb_seedjob_t)), o_queue = AL(o_seeds + nsuper * 32);
     const size_t total = AL(o_queue + 64);
 #undef AL
-    pb_munit_t *hu = (pb_munit_t *)malloc(units * sizeof(pb_munit_t));
-    pb_seedjob_t *hj = (pb_seedjob_t *)malloc(nsuper * sizeof(pb_seedjob_t));
-    if (!hu || !hj || slot_tables(wv, total) != 0) {
-        free(hu);
-        free(hj);
+    if (slot_tables(wv, total) != 0 || slot_stage(wv, o_seeds) != 0) {
         arena_give(s, off, scratch);
         return 0;
     }
+    pb_munit_t *hu = (pb_munit_t *)(wv->h_stage + o_units);
+    pb_seedjob_t *hj = (pb_seedjob_t *)(wv->h_stage + o_jobs);
     {
         uint64_t u = 0, j = 0;
         for (size_t k = 0; k < n; k++) {
@@ -337,14 +394,7 @@ static int admit_deep(pose_b200_server_t *s)
         }
     }
     uint8_t *T = (uint8_t *)wv->d_tables;
-    int ok = cudaMemcpyAsync(T + o_units, hu, units * sizeof(pb_munit_t), cudaMemcpyHostToDevice, wv->stream) ==
-             cudaSuccess;
-    ok = ok && cudaMemcpyAsync(T + o_jobs, hj, nsuper * sizeof(pb_seedjob_t), cudaMemcpyHostToDevice, wv->stream) ==
-                   cudaSuccess;
-    /* the uploads read the host tables: wait for them before freeing them */
-    ok = ok && cudaStreamSynchronize(wv->stream) == cudaSuccess;
-    free(hu);
-    free(hj);
+    int ok = cudaMemcpyAsync(T, wv->h_stage, o_seeds, cudaMemcpyHostToDevice, wv->stream) == cudaSuccess;
     ok = ok && pb_dev_seed_jobs(T + o_jobs, (uint32_t)nsuper, s->d_sessions, (uint32_t *)(T + o_seeds), wv->stream) == 0;
     ok = ok && cudaMemsetAsync(T + o_queue, 0, 64, wv->stream) == cudaSuccess;
     if (ok) {
@@ -407,7 +457,7 @@ static int admit_wave(pose_b200_server_t *s)
     uint32_t multi = 0;
     for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
         if (s->waves[i].busy) multi++;
-        else if (w < 0) w = (int)i;
+        else if (w < 0 && !chan_busy(s, s->waves[i].chan)) w = (int)i;
     }
     if (w < 0 || multi >= s->max_waves) return 0;
     wave_t *wv = &s->waves[w];
@@ -498,14 +548,18 @@ static int admit_wave(pose_b200_server_t *s)
     o_queue = AL(o_seeds + pl.njobs * 32);
     total = AL(o_queue + 64);
 #undef AL
-    if (slot_tables(wv, total) != 0) { arena_give(s, off, scratch); pb_plan_free(&pl); return 0; }
+    if (slot_tables(wv, total) != 0 || slot_stage(wv, o_seeds) != 0) {
+        arena_give(s, off, scratch);
+        pb_plan_free(&pl);
+        return 0;
+    }
     uint8_t *T = (uint8_t *)wv->d_tables;
-    int ok = 1;
-    ok &= cudaMemcpyAsync(T + o_views, pl.views, pl.ntopo * sizeof(pb_topo_view_t), cudaMemcpyHostToDevice, wv->stream) == cudaSuccess;
-    ok &= cudaMemcpyAsync(T + o_batches, pl.batches, pl.nbatches * sizeof(pb_mbatch_t), cudaMemcpyHostToDevice, wv->stream) == cudaSuccess;
-    ok &= cudaMemcpyAsync(T + o_units, pl.units, pl.nunits * sizeof(pb_munit_t), cudaMemcpyHostToDevice, wv->stream) == cudaSuccess;
-    ok &= cudaMemcpyAsync(T + o_ureq, pl.unit_req, pl.nunits * sizeof(uint32_t), cudaMemcpyHostToDevice, wv->stream) == cudaSuccess;
-    ok &= cudaMemcpyAsync(T + o_jobs, pl.jobs, pl.njobs * sizeof(pb_seedjob_t), cudaMemcpyHostToDevice, wv->stream) == cudaSuccess;
+    memcpy(wv->h_stage + o_views, pl.views, pl.ntopo * sizeof(pb_topo_view_t));
+    memcpy(wv->h_stage + o_batches, pl.batches, pl.nbatches * sizeof(pb_mbatch_t));
+    memcpy(wv->h_stage + o_units, pl.units, pl.nunits * sizeof(pb_munit_t));
+    memcpy(wv->h_stage + o_ureq, pl.unit_req, pl.nunits * sizeof(uint32_t));
+    memcpy(wv->h_stage + o_jobs, pl.jobs, pl.njobs * sizeof(pb_seedjob_t));
+    int ok = cudaMemcpyAsync(T, wv->h_stage, o_seeds, cudaMemcpyHostToDevice, wv->stream) == cudaSuccess;
     ok &= pb_dev_seed_jobs(T + o_jobs, (uint32_t)pl.njobs, s->d_sessions, (uint32_t *)(T + o_seeds), wv->stream) == 0;
     ok &= cudaMemsetAsync(T + o_queue, 0, 64, wv->stream) == cudaSuccess;
     pb_multi_params_t p;
@@ -667,6 +721,14 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
     s->free_off[0] = 0;
     s->free_len[0] = scratch_bytes;
     s->nfree = 1;
+    {
+        const char *ec = getenv("CUDA_DEVICE_MAX_CONNECTIONS");
+        s->conns = ec && atoi(ec) > 0 ? (uint32_t)atoi(ec) : 8;
+        if (s->conns > 32) s->conns = 32;
+    }
+    /* the slots' streams are created back to back: waves, then deep slots */
+    for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) s->waves[i].chan = i % s->conns;
+    for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP; i++) s->deeps[i].chan = (PB_SERVER_MAX_WAVES + i) % s->conns;
     for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
         if (cudaStreamCreateWithFlags(&s->waves[i].stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&s->waves[i].done, cudaEventDisableTiming) != cudaSuccess)
@@ -695,17 +757,17 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
         s->wsg_smem_max = ed && ed[0] == '0' ? 0 : mx;
         /* deep-request policy (tuning): queue threshold, units per CTA, wait or join a wave, SM held alone */
         s->deep_queue = PB_SERVER_DEEP_QUEUE;
-        s->deep_units = 0;
+        s->deep_units = 4;
         s->deep_gmax = 4;
-        s->deep_wait = 0;
-        s->deep_excl = 0;
+        s->deep_wait = 1;
+        s->deep_excl = 1;
         s->deep_levels = PB_SERVER_DEEP_LEVELS;
         const char *e0 = getenv("POSE_B200_SERVER_DEEP_LEVELS");
         if (e0 && atoi(e0) > 0) s->deep_levels = (uint32_t)atoi(e0);
         const char *e1 = getenv("POSE_B200_SERVER_DEEP_QUEUE");
         if (e1 && e1[0]) s->deep_queue = (uint32_t)atoi(e1);
         const char *e2 = getenv("POSE_B200_SERVER_DEEP_UNITS");
-        if (e2 && atoi(e2) >= 1 && atoi(e2) <= 4) s->deep_units = (uint32_t)atoi(e2);
+        if (e2 && atoi(e2) >= 0 && atoi(e2) <= 4) s->deep_units = (uint32_t)atoi(e2);
         const char *e3 = getenv("POSE_B200_SERVER_DEEP_GMAX");
         if (e3 && atoi(e3) >= 1 && atoi(e3) <= 4) s->deep_gmax = (uint32_t)atoi(e3);
         const char *e4 = getenv("POSE_B200_SERVER_DEEP_WAIT");
@@ -722,6 +784,7 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
     for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) {
         wave_t *wv = &s->waves[i];
         if (slot_tables(wv, (size_t)512 << 10) != 0) cudaGetLastError();
+        if (slot_stage(wv, (size_t)512 << 10) != 0) cudaGetLastError();
         if (cudaHostAlloc((void **)&wv->h_done, 4096 * sizeof(unsigned int), cudaHostAllocMapped) == cudaSuccess &&
             cudaHostGetDevicePointer((void **)&wv->d_done, wv->h_done, 0) == cudaSuccess) {
             wv->done_cap = 4096;
@@ -732,8 +795,10 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
             cudaGetLastError();
         }
     }
-    for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP; i++)
+    for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP; i++) {
         if (slot_tables(&s->deeps[i], (size_t)64 << 10) != 0) cudaGetLastError();
+        if (slot_stage(&s->deeps[i], (size_t)64 << 10) != 0) cudaGetLastError();
+    }
     s->running = 1;
     if (pthread_create(&s->thread, NULL, dispatcher, s) != 0) { s->running = 0; goto fail; }
     return s;
@@ -744,11 +809,13 @@ fail:
         if (s->waves[i].done) cudaEventDestroy(s->waves[i].done);
         cudaFree(s->waves[i].d_tables);
         if (s->waves[i].h_done) cudaFreeHost(s->waves[i].h_done);
+        if (s->waves[i].h_stage) cudaFreeHost(s->waves[i].h_stage);
     }
     for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP; i++) {
         if (s->deeps[i].stream) cudaStreamDestroy(s->deeps[i].stream);
         if (s->deeps[i].done) cudaEventDestroy(s->deeps[i].done);
         cudaFree(s->deeps[i].d_tables);
+        if (s->deeps[i].h_stage) cudaFreeHost(s->deeps[i].h_stage);
     }
     cudaFree(s->d_arena);
     pthread_mutex_destroy(&s->mu);
@@ -913,6 +980,7 @@ void pose_b200_server_destroy(pose_b200_server_t *s)
         cudaEventDestroy(wv->done);
         cudaFree(wv->d_tables);
         if (wv->h_done) cudaFreeHost(wv->h_done);
+        if (wv->h_stage) cudaFreeHost(wv->h_stage);
         free(wv->reqs);
         free(wv->need);
     }

@@ -66,15 +66,21 @@ def test_oversized_request_is_rejected(pkg, cuda):
         assert srv.submit(topo, 99, buf.data_ptr(), 4096 * 32, 0) == -1  # unknown session
 
 
-@pytest.mark.parametrize("deep_sms", [0, 8])
-def test_deep_requests_run_on_the_depth_kernel_and_match_alone(pkg, cuda, monkeypatch, deep_sms):
-    """A request at chunk_blocks 2^17 on an idle GPU runs on the depth
-    kernel, one chunk copy per CTA; deep requests that arrive with a queue,
-    or (with the depth kernel held to 8 SMs) do not fit the free SMs, join
-    the waves of shallow requests.  Every result equals labelling that
-    request alone."""
+@pytest.mark.parametrize("deep_sms,units", [(0, None), (8, "0"), (8, "1")])
+def test_deep_requests_run_on_the_depth_kernel_and_match_alone(pkg, cuda, monkeypatch, deep_sms, units):
+    """Requests at chunk_blocks 2^17 (made deep for the test) run on the
+    depth kernel: four chunk copies per CTA with the SM held alone (the
+    default); with units "0", the fewest copies per CTA that fit an idle
+    GPU; with the depth kernel held to 8 SMs, a request that does not fit
+    the free SMs waits for them, and one larger than all 8 (units "1": 10
+    copies) runs its CTAs over the batches in turn.  Shallow requests in
+    waves run beside them.  Every result equals labelling that request
+    alone."""
+    monkeypatch.setenv("POSE_B200_SERVER_DEEP_LEVELS", "300000")
     if deep_sms:
         monkeypatch.setenv("POSE_B200_SERVER_DEEP_SMS", str(deep_sms))
+    if units is not None:
+        monkeypatch.setenv("POSE_B200_SERVER_DEEP_UNITS", units)
     rnd = random.Random(17)
     deep_cb, cbs = 1 << 17, [1024, 1 << 14]
     topos = {cb: pkg.Topology(cb) for cb in [deep_cb] + cbs}
@@ -90,8 +96,7 @@ def test_deep_requests_run_on_the_depth_kernel_and_match_alone(pkg, cuda, monkey
             sessions = [srv.session(k) for k in seed_list]
             for t in topos.values():
                 srv.prepare(t)
-            # the first deep request alone (an idle GPU: the depth kernel), then
-            # the rest in a burst (deep requests that find a queue join waves)
+            # the first deep request alone (an idle GPU), then the rest in a burst
             cb, ns, rbo, sid, buf = reqs[0]
             first = srv.submit(topos[cb], sessions[sid], buf.data_ptr(), ns * cb * 32, rbo)
             assert srv.wait(first)[0] == 0
