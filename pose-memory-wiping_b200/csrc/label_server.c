@@ -22,9 +22,9 @@
  *   - finished waves are reaped and their arena range is zeroed on the device
  *     before it is reused;
  *   - deep requests (topologies of at least PB_SERVER_DEEP_LEVELS levels,
- *     chunk_blocks 2^18 and up) do not join waves: the pending deep requests
+ *     chunk_blocks 2^17 and up) do not join waves: the pending deep requests
  *     of one topology run together on the multi-unit depth kernel
- *     (k_label_wsg: a producer warp and 15 hashing warps per CTA, four chunk
+ *     (k_label_wsg: a producer warp and 15 hashing warps per CTA, three chunk
  *     copies per CTA) in a slot of their own, on a high-priority stream.
  *     Each depth CTA holds its SM alone (its shared memory is raised to the
  *     limit), so no lockstep warp slows its chain, and at most one depth CTA
@@ -58,14 +58,15 @@
 #define PB_SERVER_MAX_WAVES 16
 /* Concurrent launches of the depth kernel. */
 #define PB_SERVER_MAX_DEEP 16
-/* Requests whose topology has at least this many levels (chunk_blocks 2^18
- * and up: a chunk copy's chain alone is 2.4 s on the lockstep kernel) run on
- * the depth kernel instead of joining a wave.  On the 120-request Poisson
- * trace (200 requests/s, chunk_blocks 2^10..2^18) this served 534 MiB/s,
- * against 486 with 2^17 included (one SM per CTA holds more SM time than
- * the lockstep kernel's 2^17 chains cost) and 448 with every request in
- * waves. */
-#define PB_SERVER_DEEP_LEVELS 600000u
+/* Requests whose topology has at least this many levels (chunk_blocks 2^17
+ * and up) run on the depth kernel instead of joining a wave.  On the
+ * 120-request Poisson trace (200 requests/s, chunk_blocks 2^10..2^18), with
+ * three chunk copies per depth CTA: 603 MiB/s, against 549 with only 2^18 on
+ * the depth kernel and 448 with every request in waves. */
+#define PB_SERVER_DEEP_LEVELS 300000u
+/* Chunk copies per depth CTA under the default policy (measured on the same
+ * trace: 3 copies 549-603 MiB/s, 4 copies 515-548, 2 copies 520). */
+#define PB_SERVER_DEEP_UNITS 3u
 /* Hashing warps of a depth-kernel CTA. */
 #define PB_SERVER_DEEP_WARPS 15u
 /* A deep request joins a wave instead when more than this many requests
@@ -757,7 +758,7 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
         s->wsg_smem_max = ed && ed[0] == '0' ? 0 : mx;
         /* deep-request policy (tuning): queue threshold, units per CTA, wait or join a wave, SM held alone */
         s->deep_queue = PB_SERVER_DEEP_QUEUE;
-        s->deep_units = 4;
+        s->deep_units = PB_SERVER_DEEP_UNITS;
         s->deep_gmax = 4;
         s->deep_wait = 1;
         s->deep_excl = 1;

@@ -68,15 +68,14 @@ def test_oversized_request_is_rejected(pkg, cuda):
 
 @pytest.mark.parametrize("deep_sms,units", [(0, None), (8, "0"), (8, "1")])
 def test_deep_requests_run_on_the_depth_kernel_and_match_alone(pkg, cuda, monkeypatch, deep_sms, units):
-    """Requests at chunk_blocks 2^17 (made deep for the test) run on the
-    depth kernel: four chunk copies per CTA with the SM held alone (the
-    default); with units "0", the fewest copies per CTA that fit an idle
-    GPU; with the depth kernel held to 8 SMs, a request that does not fit
-    the free SMs waits for them, and one larger than all 8 (units "1": 10
-    copies) runs its CTAs over the batches in turn.  Shallow requests in
-    waves run beside them.  Every result equals labelling that request
-    alone."""
-    monkeypatch.setenv("POSE_B200_SERVER_DEEP_LEVELS", "300000")
+    """Requests at chunk_blocks 2^17 run on the depth kernel: three chunk
+    copies per CTA with the SM held alone (the default: 2 and 5 chunks make
+    ragged last batches); with units "0", the fewest copies per CTA that fit
+    an idle GPU; with the depth kernel held to 8 SMs, a request that does
+    not fit the free SMs waits for them, and one larger than all 8 (units
+    "1": 10 copies) runs its CTAs over the batches in turn.  Shallow
+    requests in waves run beside them.  Every result equals labelling that
+    request alone."""
     if deep_sms:
         monkeypatch.setenv("POSE_B200_SERVER_DEEP_SMS", str(deep_sms))
     if units is not None:
