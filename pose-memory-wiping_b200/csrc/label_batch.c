@@ -48,14 +48,14 @@ typedef struct {
 
 struct pose_b200_batch {
     int device;
-    cudaStream_t stream, stream2;
+    cudaStream_t stream, stream2, stream3;
     cudaGraph_t graph;
     cudaGraphExec_t exec;
-    cudaEvent_t ev[6]; /* 0/3: replay start/end; 1/2: first launch's kernel; 4/5: fork/join */
+    cudaEvent_t ev[8]; /* 0/3: replay start/end; 1/2: first launch's kernel; 4/5, 6/7: fork/join */
     void *d_blob; /* the requests' session seeds, back to back */
     size_t blob_len;
     int nparts;
-    batch_part_t part[2]; /* part[1]: the deep requests, when split */
+    batch_part_t part[3]; /* part[1]: the deep requests, when split; part[2]: the next-deepest topology's */
     uint64_t scratch_bytes, nodes, super_chunks, units;
     uint32_t nbatches, teams, T, Gmax, fma, cv0;
 };
@@ -86,13 +86,14 @@ static void batch_free(pose_b200_batch_t *b)
     }
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < 3; i++) {
         batch_part_t *q = &b->part[i];
         cudaFree(q->d_topos); cudaFree(q->d_batches); cudaFree(q->d_units); cudaFree(q->d_jobs);
         cudaFree(q->d_seeds); cudaFree(q->d_scratch); cudaFree(q->d_queue);
     }
     cudaFree(b->d_blob);
-    for (int i = 0; i < 6; i++) if (b->ev[i]) cudaEventDestroy(b->ev[i]);
+    for (int i = 0; i < 8; i++) if (b->ev[i]) cudaEventDestroy(b->ev[i]);
+    if (b->stream3) cudaStreamDestroy(b->stream3);
     if (b->stream2) cudaStreamDestroy(b->stream2);
     if (b->stream) cudaStreamDestroy(b->stream);
     free(b);
@@ -348,6 +349,36 @@ static size_t split_deep(const pb_req_t *pr, size_t n, uint8_t *deep)
     return nd;
 }
 
+/* The second deep part: among the requests split_deep left shallow, those of
+ * the deepest remaining topology, when its chain (8-warp team, one unit) is
+ * at least a third of the deepest request's.  They are marked 2 in `deep`;
+ * returns how many. */
+static size_t split_second(const pb_req_t *pr, size_t n, uint8_t *deep)
+{
+    uint64_t maxc = 0, c2 = 0;
+    const pose_hbm_topo_t *t2 = NULL;
+    for (size_t i = 0; i < n; i++) {
+        pb_topo_internal_t x;
+        if (pb_topo_internal(pr[i].topo, &x) != 0 || pr[i].len < x.super_bytes) continue;
+        const uint64_t c = pb_topo_passes(pr[i].topo, 8, 1);
+        if (c > maxc) maxc = c;
+        if (!deep[i] && c > c2) {
+            c2 = c;
+            t2 = pr[i].topo;
+        }
+    }
+    if (!t2 || 3 * c2 < maxc) return 0;
+    size_t n2 = 0;
+    for (size_t i = 0; i < n; i++) {
+        pb_topo_internal_t x;
+        if (deep[i] || pr[i].topo != t2 || pb_topo_internal(pr[i].topo, &x) != 0 || pr[i].len < x.super_bytes)
+            continue;
+        deep[i] = 2;
+        n2++;
+    }
+    return n2;
+}
+
 /* Size, allocate and upload one launch of a batch; `slots` caps its resident
  * threads in units of 256 (256 / 32T teams each) and `budget` its scratch.
  * One team per CTA.  Returns 0, or -1 (message on stderr). */
@@ -504,11 +535,11 @@ pose_b200_batch_t *pose_b200_batch_create(const pose_b200_request_t *reqs, size_
                                           const pose_b200_sched_t *sched)
 {
     pose_b200_batch_t *b = NULL;
-    pb_req_t *pr = NULL, *pd = NULL, *ps = NULL;
+    pb_req_t *pr = NULL, *pd = NULL, *pd2 = NULL, *ps = NULL;
     uint8_t *blob = NULL, *deep = NULL;
-    pb_plan_tables_t pl[2];
+    pb_plan_tables_t pl[3];
     memset(pl, 0, sizeof(pl));
-    size_t blob_len = 0, nd = 0, ns = 0;
+    size_t blob_len = 0, nd = 0, nd2 = 0, ns = 0;
     int dev = -1;
 
     if (!reqs || n == 0) { fprintf(stderr, "pose_b200_batch_create: no requests\n"); return NULL; }
@@ -528,10 +559,11 @@ pose_b200_batch_t *pose_b200_batch_create(const pose_b200_request_t *reqs, size_
     }
     pr = (pb_req_t *)calloc(n, sizeof(*pr));
     pd = (pb_req_t *)calloc(n, sizeof(*pd));
+    pd2 = (pb_req_t *)calloc(n, sizeof(*pd2));
     ps = (pb_req_t *)calloc(n, sizeof(*ps));
     deep = (uint8_t *)calloc(n, 1);
     blob = (uint8_t *)malloc(blob_len ? blob_len : 1);
-    if (!pr || !pd || !ps || !deep || !blob) goto fail_host;
+    if (!pr || !pd || !pd2 || !ps || !deep || !blob) goto fail_host;
     {
         uint64_t off = 0;
         for (size_t i = 0; i < n; i++) {
@@ -549,11 +581,16 @@ pose_b200_batch_t *pose_b200_batch_create(const pose_b200_request_t *reqs, size_
     if (!(sched && (sched->flags & POSE_B200_BATCH_ONE_LAUNCH))) {
         for (size_t i = 0; i < n; i++) if (!pr[i].topo) goto no_split;
         nd = split_deep(pr, n, deep);
+        /* POSE_B200_DEEP2=0 keeps the next-deepest topology with the rest */
+        const char *e2 = getenv("POSE_B200_DEEP2");
+        if (nd && !(e2 && e2[0] == '0')) nd2 = split_second(pr, n, deep);
     }
 no_split:
     if (nd) {
+        size_t a = 0, c = 0;
         for (size_t i = 0; i < n; i++) {
-            if (deep[i]) pd[i - ns] = pr[i];
+            if (deep[i] == 1) pd[a++] = pr[i];
+            else if (deep[i] == 2) pd2[c++] = pr[i];
             else ps[ns++] = pr[i];
         }
     } else {
@@ -566,7 +603,8 @@ no_split:
     b->device = dev;
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
     if (nd && cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking) != cudaSuccess) goto fail;
-    for (int i = 0; i < 6; i++) if (cudaEventCreate(&b->ev[i]) != cudaSuccess) goto fail;
+    if (nd2 && cudaStreamCreateWithFlags(&b->stream3, cudaStreamNonBlocking) != cudaSuccess) goto fail;
+    for (int i = 0; i < 8; i++) if (cudaEventCreate(&b->ev[i]) != cudaSuccess) goto fail;
     b->blob_len = blob_len;
     if (pb_dev_malloc(&b->d_blob, blob_len ? blob_len : 1) != cudaSuccess) {
         fprintf(stderr, "pose_b200_batch_create: alloc: %s\n", cudaGetErrorString(cudaGetLastError()));
@@ -622,6 +660,40 @@ no_split:
                 const uint32_t smem = pb_wsg_smem_bytes(v2.csm, G, 15);
                 if (pb_plan_requests(pd, nd, 8, 1, 0.9999, &pl[1]) != 0 || pl[1].nunits == 0) goto fail;
                 if (part_setup_wsg(b, &b->part[1], &pl[1], &v2, G, sms, smem) != 0) goto fail;
+                /* the next-deepest topology's requests: a third launch of the
+                 * depth kernel on the SMs the first leaves, its CTAs looping
+                 * over their batches */
+                if (nd2) {
+                    pb_topo_view2_t v2b;
+                    uint64_t du2 = 0;
+                    for (size_t i = 0; i < nd2; i++) {
+                        pb_topo_internal_t x;
+                        if (pb_topo_internal(pd2[i].topo, &x) != 0) goto fail;
+                        du2 += (uint64_t)(pd2[i].len / x.super_bytes) * x.copies;
+                    }
+                    uint32_t G2 = 4;
+                    const char *eu = getenv("POSE_B200_DEEP2_UNITS"); /* tuning: copies per CTA, 1 to 4 */
+                    if (eu && eu[0] >= '1' && eu[0] <= '4' && !eu[1]) G2 = (uint32_t)(eu[0] - '0');
+                    const uint32_t left = sms > b->part[1].grid ? sms - b->part[1].grid : 0;
+                    uint32_t max_smem2 = 0;
+                    int ok2 = left > 0 && pb_topo_view2_small(pd2[0].topo, &v2b) == 0 &&
+                              pb_dev_label_wsg_prepare(&max_smem2) == 0 &&
+                              pb_wsg_smem_bytes(v2b.csm, G2, 15) <= max_smem2;
+                    cudaGetLastError();
+                    if (ok2) {
+                        const uint64_t g2 = (du2 + G2 - 1) / G2 < left ? (du2 + G2 - 1) / G2 : left;
+                        ok2 = b->part[1].scratch_bytes + g2 * ((uint64_t)v2b.gpool * 32 * G2) <= budget;
+                    }
+                    if (ok2) {
+                        if (pb_plan_requests(pd2, nd2, 8, 1, 0.9999, &pl[2]) != 0 || pl[2].nunits == 0) goto fail;
+                        if (part_setup_wsg(b, &b->part[2], &pl[2], &v2b, G2, left, pb_wsg_smem_bytes(v2b.csm, G2, 15)) !=
+                            0)
+                            goto fail;
+                    } else {
+                        for (size_t i = 0; i < nd2; i++) ps[ns++] = pd2[i];
+                        nd2 = 0;
+                    }
+                }
             } else {
                 uint32_t g = 1;
                 while (g < 4 && 2 * (dunits + g - 1) / g > (uint64_t)sms * occ) g *= 2;
@@ -630,7 +702,12 @@ no_split:
                 if (deep_ctas * 2 > (uint64_t)pl[1].sms * occ) deep_ctas = (uint64_t)pl[1].sms * occ / 2;
                 if (part_setup(b, &b->part[1], &pl[1], 8, deep_ctas, budget, NULL) != 0) goto fail;
             }
-            budget = budget > b->part[1].scratch_bytes ? budget - b->part[1].scratch_bytes : 0;
+            if (nd2 && !wsg) { /* the lockstep deep part: the next-deepest requests stay with the rest */
+                for (size_t i = 0; i < nd2; i++) ps[ns++] = pd2[i];
+                nd2 = 0;
+            }
+            const uint64_t used = b->part[1].scratch_bytes + (nd2 ? b->part[2].scratch_bytes : 0);
+            budget = budget > used ? budget - used : 0;
         }
         const uint32_t gcap = sched && sched->units_per_team ? sched->units_per_team : 32;
         uint32_t T = 4;
@@ -639,11 +716,14 @@ no_split:
         if (pb_plan_requests(ps, ns, T, gcap, eff, &pl[0]) != 0) goto fail;
         if (pl[0].nunits == 0 && !nd) { fprintf(stderr, "pose_b200_batch_create: no super-chunk to label\n"); goto fail; }
         slots = (uint64_t)pl[0].sms * occ;
-        slots = slots > b->part[1].grid ? slots - b->part[1].grid : 1;
+        {
+            const uint64_t taken = (uint64_t)b->part[1].grid + (nd2 ? b->part[2].grid : 0);
+            slots = slots > taken ? slots - taken : 1;
+        }
         if (pl[0].nunits) {
             if (part_setup(b, &b->part[0], &pl[0], T, slots, budget, sched) != 0) goto fail;
         }
-        b->nparts = nd ? 2 : 1;
+        b->nparts = nd2 ? 3 : nd ? 2 : 1;
         b->T = T;
         for (int i = 0; i < b->nparts; i++) {
             const batch_part_t *q = &b->part[i];
@@ -655,7 +735,7 @@ no_split:
             b->scratch_bytes += q->scratch_bytes;
             if (q->Gmax > b->Gmax) b->Gmax = q->Gmax;
         }
-        b->cv0 = (pl[0].nunits == 0 || b->part[0].cv0) && (!nd || b->part[1].cv0);
+        b->cv0 = (pl[0].nunits == 0 || b->part[0].cv0) && (!nd || b->part[1].cv0) && (!nd2 || b->part[2].cv0);
 
         /* capture: the rest on the batch's stream; the deep part forked onto
          * a second stream and joined back */
@@ -667,8 +747,15 @@ no_split:
             if (crc == 0) crc = part_capture(b, &b->part[1], b->stream2, NULL, NULL);
             if (crc == 0) crc = cudaEventRecord(b->ev[5], b->stream2) == cudaSuccess ? 0 : -1;
         }
+        if (crc == 0 && nd2) {
+            crc = cudaEventRecord(b->ev[6], b->stream) == cudaSuccess ? 0 : -1;
+            if (crc == 0) crc = cudaStreamWaitEvent(b->stream3, b->ev[6], 0) == cudaSuccess ? 0 : -1;
+            if (crc == 0) crc = part_capture(b, &b->part[2], b->stream3, NULL, NULL);
+            if (crc == 0) crc = cudaEventRecord(b->ev[7], b->stream3) == cudaSuccess ? 0 : -1;
+        }
         if (crc == 0 && pl[0].nunits) crc = part_capture(b, &b->part[0], b->stream, b->ev[1], b->ev[2]);
         if (crc == 0 && nd) crc = cudaStreamWaitEvent(b->stream, b->ev[5], 0) == cudaSuccess ? 0 : -1;
+        if (crc == 0 && nd2) crc = cudaStreamWaitEvent(b->stream, b->ev[7], 0) == cudaSuccess ? 0 : -1;
         cudaError_t ce = cudaStreamEndCapture(b->stream, &b->graph);
         if (crc != 0 || ce != cudaSuccess) {
             fprintf(stderr, "pose_b200_batch_create: graph capture failed: %s\n",
@@ -681,7 +768,8 @@ no_split:
         }
     }
     if (blob) explicit_bzero(blob, blob_len);
-    free(pr); free(pd); free(ps); free(deep); free(blob); pb_plan_free(&pl[0]); pb_plan_free(&pl[1]);
+    free(pr); free(pd); free(pd2); free(ps); free(deep); free(blob);
+    pb_plan_free(&pl[0]); pb_plan_free(&pl[1]); pb_plan_free(&pl[2]);
     return b;
 fail:
     batch_free(b);
@@ -689,7 +777,8 @@ fail:
 fail_host:
     cudaGetLastError();
     if (blob) explicit_bzero(blob, blob_len);
-    free(pr); free(pd); free(ps); free(deep); free(blob); pb_plan_free(&pl[0]); pb_plan_free(&pl[1]);
+    free(pr); free(pd); free(pd2); free(ps); free(deep); free(blob);
+    pb_plan_free(&pl[0]); pb_plan_free(&pl[1]); pb_plan_free(&pl[2]);
     return NULL;
 }
 

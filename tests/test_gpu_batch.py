@@ -154,6 +154,43 @@ def test_multi_unit_depth_kernel_writes_the_same_bytes(pkg, cuda, monkeypatch, d
             t.free()
 
 
+def test_next_deepest_topology_runs_as_a_third_launch(pkg, cuda, monkeypatch):
+    """With three topologies, the deepest one's requests and those of the
+    next-deepest (its chain at least a third as long) each run on the
+    multi-unit depth kernel (the second on the SMs the first leaves, four
+    copies per CTA, a ragged last batch); the rest in the lockstep launch.
+    The bytes equal single calls and the two-launch form
+    (POSE_B200_DEEP2=0).  The 256-session workload below runs the second
+    part's CTAs over more batches than CTAs."""
+    rnd = random.Random(23)
+    cbs = (4096, 2048, 256)
+    topos = {cb: pkg.Topology(cb) for cb in cbs}
+    try:
+        reqs, bufs = [], []
+        for i, (cb, ns) in enumerate([(4096, 2), (2048, 3), (256, 2), (2048, 2), (4096, 1), (256, 1), (2048, 2)]):
+            key = rnd.randbytes([32, 7, 32, 100, 32, 1, 32][i])
+            buf = cuda.zeros(ns * cb * 32, dtype=cuda.uint8, device="cuda")
+            reqs.append((topos[cb], key, buf.data_ptr(), ns * cb * 32, cb * rnd.randrange(1 << 20)))
+            bufs.append(buf)
+        got = {}
+        for deep2, launches in (("1", 6), ("0", 4)):
+            monkeypatch.setenv("POSE_B200_DEEP2", deep2)
+            for t in bufs:
+                t.fill_(0x4D)
+            with pkg.Batch(reqs) as b:
+                rc, st = b.run()
+            assert rc == 0 and st["kernel_launches"] == launches, (deep2, st)
+            got[deep2] = [t.cpu().numpy().tobytes() for t in bufs]
+        assert got["1"] == got["0"]
+        for (topo, key, ptr, nbytes, rbo), data in zip(reqs, got["1"]):
+            ref = cuda.full((nbytes,), 0x4D, dtype=cuda.uint8, device="cuda")
+            assert topo.label(key, ref.data_ptr(), nbytes, rbo) == 0
+            assert ref.cpu().numpy().tobytes() == data
+    finally:
+        for t in topos.values():
+            t.free()
+
+
 def test_batched_256_sessions_sampled_vs_reference(pkg, cuda, wl):
     rows = {r["session"]: r for r in golden("configs.json")["batched_sampled"]}
     sessions = wl.batched()
