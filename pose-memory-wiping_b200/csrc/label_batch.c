@@ -661,8 +661,8 @@ no_split:
                 if (pb_plan_requests(pd, nd, 8, 1, 0.9999, &pl[1]) != 0 || pl[1].nunits == 0) goto fail;
                 if (part_setup_wsg(b, &b->part[1], &pl[1], &v2, G, sms, smem) != 0) goto fail;
                 /* the next-deepest topology's requests: a third launch of the
-                 * depth kernel on the SMs the first leaves, its CTAs looping
-                 * over their batches */
+                 * depth kernel on the SMs the first leaves, three copies per
+                 * CTA, its CTAs looping over their batches */
                 if (nd2) {
                     pb_topo_view2_t v2b;
                     uint64_t du2 = 0;
@@ -671,7 +671,7 @@ no_split:
                         if (pb_topo_internal(pd2[i].topo, &x) != 0) goto fail;
                         du2 += (uint64_t)(pd2[i].len / x.super_bytes) * x.copies;
                     }
-                    uint32_t G2 = 4;
+                    uint32_t G2 = 3; /* on the 256-session workload: 3 copies 999 MiB/s, 4 copies 839-845 */
                     const char *eu = getenv("POSE_B200_DEEP2_UNITS"); /* tuning: copies per CTA, 1 to 4 */
                     if (eu && eu[0] >= '1' && eu[0] <= '4' && !eu[1]) G2 = (uint32_t)(eu[0] - '0');
                     const uint32_t left = sms > b->part[1].grid ? sms - b->part[1].grid : 0;

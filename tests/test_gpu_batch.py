@@ -157,7 +157,7 @@ def test_multi_unit_depth_kernel_writes_the_same_bytes(pkg, cuda, monkeypatch, d
 def test_next_deepest_topology_runs_as_a_third_launch(pkg, cuda, monkeypatch):
     """With three topologies, the deepest one's requests and those of the
     next-deepest (its chain at least a third as long) each run on the
-    multi-unit depth kernel (the second on the SMs the first leaves, four
+    multi-unit depth kernel (the second on the SMs the first leaves, three
     copies per CTA, a ragged last batch); the rest in the lockstep launch.
     The bytes equal single calls and the two-launch form
     (POSE_B200_DEEP2=0).  The 256-session workload below runs the second
