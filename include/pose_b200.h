@@ -191,14 +191,24 @@ int pose_b200_label_stream(const pose_hbm_topo_t *topo, const uint8_t *session_s
  * the device:
  *   - requests of deep topologies (chunk_blocks 2^17 and up) run on the
  *     multi-unit depth kernel, the pending ones of one topology together,
- *     1 to 4 chunk copies per CTA as the free SMs allow, at most one such
- *     CTA per SM, on high-priority streams;
+ *     three chunk copies per CTA, each CTA holding its SM alone, on
+ *     high-priority streams; one that does not fit the free SMs waits;
  *   - the others run in waves: one persistent multi-topology launch per
  *     wave on its own stream, a request completing as soon as its chunk
  *     copies are in;
- *   - a request that waits for SMs or scratch never holds back the others.
- * Each result is byte-identical to labelling the request alone.  All
- * topologies and buffers must be on the device that was current at
+ *   - a request that waits for SMs or scratch never holds back the others,
+ *     and the dispatcher never waits for the GPU.
+ * Launches run on streams of their own; a launch starts only where no
+ * running launch shares its host-to-device work queue, so
+ * CUDA_DEVICE_MAX_CONNECTIONS (8 by default; 32 gives every slot its own)
+ * bounds how many run at once.  Tuning variables, read at creation:
+ * POSE_B200_SERVER_DEEP_LEVELS (levels from which a topology is deep),
+ * POSE_B200_SERVER_DEEP_UNITS (copies per depth CTA; 0 = the fewest that fit
+ * an idle GPU), POSE_B200_SERVER_DEEP_EXCL and POSE_B200_SERVER_DEEP_WAIT
+ * (0: share SMs; 0: join a wave instead of waiting), POSE_B200_SERVER_DEEP=0
+ * (every request in waves), POSE_B200_SERVER_DEEP_SMS (SMs the depth kernel
+ * may hold).  Each result is byte-identical to labelling the request alone.
+ * All topologies and buffers must be on the device that was current at
  * creation. */
 typedef struct pose_b200_server pose_b200_server_t;
 
