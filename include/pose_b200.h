@@ -137,7 +137,11 @@ typedef struct pose_b200_batch pose_b200_batch_t;
  * Otherwise it is the lockstep kernel with 8-warp teams, units packed up to
  * 4 a team so that they hold about half the SMs' team slots.  The
  * environment variable POSE_B200_DEEP_KERNEL=0 selects the lockstep kernel
- * in every case. */
+ * in every case.  With the multi-unit depth kernel, the requests of the
+ * deepest remaining topology, when its chain is at least a third of the
+ * deepest, run as a third launch of it (three chunk copies per CTA, on the
+ * SMs the second launch leaves, its CTAs looping over their batches);
+ * POSE_B200_DEEP2=0 keeps them with the rest. */
 pose_b200_batch_t *pose_b200_batch_create(const pose_b200_request_t *reqs, size_t n,
                                           const pose_b200_sched_t *sched);
 /* The empirical autotuner: rank the schedules sched leaves open (team size
