@@ -701,10 +701,11 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
     pose_b200_server_t *s = (pose_b200_server_t *)calloc(1, sizeof(*s));
     if (!s) return NULL;
     cudaGetDevice(&s->device);
-    /* 3 by default: on a 120-request Poisson trace (200 requests/s, chunk_blocks
-     * 2^10..2^18) 2-3 concurrent waves served 319-342 MiB/s, 4 waves 280-323,
-     * 8 waves 278 and 16 waves 214, at equal or better p50/p99: fewer slots
-     * let arrivals gather into larger, better-packed waves */
+    /* 3 by default: on the 120-request Poisson trace (200 requests/s,
+     * chunk_blocks 2^10..2^18, deep requests on the depth kernel) 3 waves
+     * served 589-602 MiB/s (p50 1.45 s), 5 waves 593-594 (p50 1.25-1.35 s)
+     * and 8 waves 578 (p50 1.15 s); with the default 8 work queues, every
+     * wave slot in use is one fewer concurrent depth-kernel launch */
     s->max_waves = max_waves ? (max_waves < PB_SERVER_MAX_WAVES ? max_waves : PB_SERVER_MAX_WAVES) : 3;
     pthread_mutex_init(&s->mu, NULL);
     pthread_cond_init(&s->cv, NULL);
