@@ -448,7 +448,10 @@ def run_served(pkg, torch, requests: int = 300, alone: bool = False, rate: float
     out = {"workload": f"served: Poisson {rate:.4g} req/s, 64 sessions, {len(trace)} requests, chunk_blocks 2^10..2^18",
            "value": sum(sizes) / MIB / wall, "unit": "MiB/s", "p50_ms": lat_sorted[len(lat) // 2],
            "p99_ms": lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))], "waves": st["waves"],
-           "offered_mib_s": sum(sizes) / MIB / trace[-1]["arrival_s"], "wall_s": wall}
+           "offered_mib_s": sum(sizes) / MIB / trace[-1]["arrival_s"], "wall_s": wall,
+           "policy": "chunk_blocks 2^17 and up on the depth kernel (3 copies per CTA, SM held alone), "
+                     "the rest in up to 3 concurrent lockstep waves",
+           "work_queues": int(os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS", "8"))}
     if alone:
         # one request at a time, FIFO, on the same arrival times
         sub = trace
