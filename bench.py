@@ -450,7 +450,7 @@ def run_served(pkg, torch, requests: int = 300, alone: bool = False, rate: float
            "p99_ms": lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))], "waves": st["waves"],
            "offered_mib_s": sum(sizes) / MIB / trace[-1]["arrival_s"], "wall_s": wall,
            "policy": "chunk_blocks 2^17 and up on the depth kernel (3 copies per CTA, SM held alone), "
-                     "the rest in up to 3 concurrent lockstep waves",
+                     "the rest in up to 5 concurrent lockstep waves (3 with fewer than 16 work queues)",
            "work_queues": int(os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS", "8"))}
     if alone:
         # one request at a time, FIFO, on the same arrival times

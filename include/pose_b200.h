@@ -217,7 +217,8 @@ int pose_b200_label_stream(const pose_hbm_topo_t *topo, const uint8_t *session_s
 typedef struct pose_b200_server pose_b200_server_t;
 
 /* scratch_bytes: HBM arena for all waves (0 = half the free memory);
- * max_waves: concurrent waves (0 = 3, at most 16).  NULL on error. */
+ * max_waves: concurrent waves (0 = 5 when CUDA_DEVICE_MAX_CONNECTIONS is 16
+ * or more, else 3; at most 16).  NULL on error. */
 pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max_waves);
 /* Register a session seed (<= 1016 bytes); returns its id, or -1. */
 int pose_b200_server_session(pose_b200_server_t *server, const uint8_t *seed, size_t seed_len);

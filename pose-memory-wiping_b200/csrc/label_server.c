@@ -701,12 +701,19 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
     pose_b200_server_t *s = (pose_b200_server_t *)calloc(1, sizeof(*s));
     if (!s) return NULL;
     cudaGetDevice(&s->device);
-    /* 3 by default: on the 120-request Poisson trace (200 requests/s,
-     * chunk_blocks 2^10..2^18, deep requests on the depth kernel) 3 waves
-     * served 589-602 MiB/s (p50 1.45 s), 5 waves 593-594 (p50 1.25-1.35 s)
-     * and 8 waves 578 (p50 1.15 s); with the default 8 work queues, every
-     * wave slot in use is one fewer concurrent depth-kernel launch */
-    s->max_waves = max_waves ? (max_waves < PB_SERVER_MAX_WAVES ? max_waves : PB_SERVER_MAX_WAVES) : 3;
+    {
+        const char *ec = getenv("CUDA_DEVICE_MAX_CONNECTIONS");
+        s->conns = ec && atoi(ec) > 0 ? (uint32_t)atoi(ec) : 8;
+        if (s->conns > 32) s->conns = 32;
+    }
+    /* By default 5 waves with 16 or more work queues, 3 with fewer: on the
+     * 120-request Poisson trace (200 requests/s, chunk_blocks 2^10..2^18,
+     * deep requests on the depth kernel, 32 queues) 3 waves served 589-603
+     * MiB/s (p50 1.43-1.48 s), 5 waves 593-594 (p50 1.25-1.35 s) and 8 waves
+     * 578 (p50 1.15 s); with the default 8 queues every wave slot in use is
+     * one fewer concurrent depth-kernel launch */
+    s->max_waves = max_waves ? (max_waves < PB_SERVER_MAX_WAVES ? max_waves : PB_SERVER_MAX_WAVES)
+                             : (s->conns >= 16 ? 5 : 3);
     pthread_mutex_init(&s->mu, NULL);
     pthread_cond_init(&s->cv, NULL);
     if (scratch_bytes == 0) {
@@ -723,11 +730,6 @@ pose_b200_server_t *pose_b200_server_create(uint64_t scratch_bytes, uint32_t max
     s->free_off[0] = 0;
     s->free_len[0] = scratch_bytes;
     s->nfree = 1;
-    {
-        const char *ec = getenv("CUDA_DEVICE_MAX_CONNECTIONS");
-        s->conns = ec && atoi(ec) > 0 ? (uint32_t)atoi(ec) : 8;
-        if (s->conns > 32) s->conns = 32;
-    }
     /* the slots' streams are created back to back: waves, then deep slots */
     for (uint32_t i = 0; i < PB_SERVER_MAX_WAVES; i++) s->waves[i].chan = i % s->conns;
     for (uint32_t i = 0; i < PB_SERVER_MAX_DEEP; i++) s->deeps[i].chan = (PB_SERVER_MAX_WAVES + i) % s->conns;
